@@ -1,0 +1,489 @@
+// C ABI (include/epik2.h): contexts, resident datasets, the plain search and the
+// parity/inspection entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/epik2.h"
+#include "epik2_internal.h"
+
+using namespace epik2;
+
+struct epik2_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaDeviceProp prop{};
+  std::string last_error;
+  std::map<int32_t, std::unique_ptr<DevDataset>> datasets;
+  int32_t next_id = 1;
+  // search scratch
+  int scan_blocks = 0;
+  unsigned long long* d_counter = nullptr;
+  BestSlot* d_slots = nullptr;  // one per warp of the scan grid
+  BestSlot* d_best = nullptr;
+  BestSlot* d_cand = nullptr;   // 32 per warp (top-k form)
+  int64_t* d_pgoff = nullptr;
+  int64_t pgoff_cap = 0;
+  BestSlot* h_best = nullptr;   // pinned
+  // last top-k result
+  std::vector<epik2_best> last_topk;
+};
+
+namespace {
+
+int fail(epik2_ctx* ctx, int status, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return status;
+}
+
+int cuda_fail(epik2_ctx* ctx, cudaError_t e, const char* what) {
+  std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return fail(ctx, EPIK2_E_NOMEM, msg);
+  return fail(ctx, EPIK2_E_CUDA, msg);
+}
+
+#define CK(ctx, call, what)                                  \
+  do {                                                       \
+    cudaError_t _e = (call);                                 \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, what);  \
+  } while (0)
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct Layout {
+  size_t geno, perm, planes, singles, pairs, lut, total;
+};
+
+Layout dataset_layout(int64_t s, int64_t m) {
+  const int64_t m_pad = (m + 31) / 32 * 32;
+  const int64_t words = (s + 31) / 32 + 1;  // enough for any class split
+  Layout L{};
+  size_t off = 0;
+  L.geno = off;
+  off = align_up(off + (size_t)(s * m), 256);
+  L.perm = off;
+  off = align_up(off + (size_t)s * 4, 256);
+  L.planes = off;
+  off = align_up(off + (size_t)(words * m_pad) * 8, 256);
+  L.singles = off;
+  off = align_up(off + (size_t)m_pad * 16, 256);
+  L.pairs = off;
+  off = align_up(off + (size_t)(2 * tri_size(m_pad)) * 16, 256);
+  L.lut = off;
+  off = align_up(off + (size_t)(s + 2) * 4, 256);
+  L.total = off;
+  return L;
+}
+
+// Class-sorted sample order (controls, then cases) and the case count.
+int64_t make_perm(const uint8_t* pheno, int64_t s, std::vector<int32_t>& perm) {
+  perm.resize((size_t)s);
+  int64_t n1 = 0;
+  for (int64_t t = 0; t < s; t++) n1 += (pheno[t] == 1);
+  int64_t c0 = 0, c1 = s - n1;
+  for (int64_t t = 0; t < s; t++) {
+    if (pheno[t] == 1) perm[(size_t)c1++] = (int32_t)t;
+    else perm[(size_t)c0++] = (int32_t)t;
+  }
+  return n1;
+}
+
+int encode_with(epik2_ctx* ctx, DevDataset& d, const uint8_t* pheno) {
+  std::vector<int32_t> perm;
+  d.n_cases = make_perm(pheno, d.n_samples, perm);
+  d.n_controls = d.n_samples - d.n_cases;
+  d.w0 = (d.n_controls + 31) / 32;
+  d.w1 = (d.n_cases + 31) / 32;
+  CK(ctx, cudaMemcpyAsync(d.perm, perm.data(), perm.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "upload perm");
+  CK(ctx, launch_encode(d, ctx->stream), "encode kernel");
+  CK(ctx, launch_counts(d, ctx->stream), "count kernels");
+  CK(ctx, cudaStreamSynchronize(ctx->stream), "encode");
+  return EPIK2_OK;
+}
+
+DevDataset* find(epik2_ctx* ctx, int32_t id) {
+  auto it = ctx->datasets.find(id);
+  return it == ctx->datasets.end() ? nullptr : it->second.get();
+}
+
+void decode_key(unsigned long long key, uint32_t& i, uint32_t& j, uint32_t& k) {
+  i = (uint32_t)(key >> 42);
+  j = (uint32_t)((key >> 21) & ((1ull << 21) - 1));
+  k = (uint32_t)(key & ((1ull << 21) - 1));
+}
+
+int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
+  if (n <= ctx->pgoff_cap) return EPIK2_OK;
+  if (ctx->d_pgoff) cudaFree(ctx->d_pgoff);
+  ctx->d_pgoff = nullptr;
+  ctx->pgoff_cap = 0;
+  CK(ctx, cudaMalloc(&ctx->d_pgoff, (size_t)n * 8), "alloc pair-group offsets");
+  ctx->pgoff_cap = n;
+  return EPIK2_OK;
+}
+
+// Pair groups of first index i: j0 = i+1, i+5, ... while j0 <= m-2.
+int64_t groups_of(int64_t m, int64_t i) { return (i <= m - 3) ? (m - 2 - i + kPairsPerWarp) / kPairsPerWarp : 0; }
+
+int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* dump_tables, float* dump_scores,
+             BestSlot* best_out) {
+  const int64_t m = d.n_snps;
+  int64_t ib = 0, ie = m;
+  int top_k = 0;
+  if (opts) {
+    if (opts->snp_begin != 0 || opts->snp_end != 0) {
+      ib = std::max<int64_t>(0, opts->snp_begin);
+      ie = std::min<int64_t>(m, opts->snp_end);
+    }
+    if (opts->top_k < 0 || opts->top_k > 32) return fail(ctx, EPIK2_E_INVALID, "top_k must be in [0, 32]");
+    top_k = opts->top_k;
+    if (opts->engine != 0 && opts->engine != 1) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
+  }
+  if (ie < ib) ie = ib;
+  const int64_t n_first = std::max<int64_t>(ie - ib, 1);
+  std::vector<int64_t> off((size_t)n_first + 1, 0);
+  for (int64_t t = 0; t < n_first; t++) off[(size_t)t + 1] = off[(size_t)t] + (ib + t < ie ? groups_of(m, ib + t) : 0);
+  int r = ensure_pgoff(ctx, n_first + 1);
+  if (r) return r;
+  CK(ctx, cudaMemcpyAsync(ctx->d_pgoff, off.data(), off.size() * 8, cudaMemcpyHostToDevice, ctx->stream),
+     "upload pair-group offsets");
+  CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream), "reset counter");
+  ScanParams p{};
+  p.planes = d.planes;
+  p.singles = d.singles;
+  p.pairs = d.pairs;
+  p.lut = d.lut;
+  p.pg_off = ctx->d_pgoff;
+  p.n_groups = off.back();
+  p.tri = d.tri;
+  p.n_first = (int32_t)n_first;
+  p.i_begin = (int32_t)ib;
+  p.m = (int32_t)m;
+  p.m_pad = (int32_t)d.m_pad;
+  p.w0 = (int32_t)d.w0;
+  p.w1 = (int32_t)d.w1;
+  p.n0 = (int32_t)d.n_controls;
+  p.n1 = (int32_t)d.n_cases;
+  p.counter = ctx->d_counter;
+  p.slots = ctx->d_slots;
+  p.top_k = top_k;
+  p.cand = ctx->d_cand;
+  p.dump_tables = dump_tables;
+  p.dump_scores = dump_scores;
+  const bool dump = dump_tables != nullptr;
+  CK(ctx, launch_scan_int(p, ctx->scan_blocks, dump, ctx->stream), "scan kernel");
+  const int n_warps = ctx->scan_blocks * (kScanThreads / 32);
+  CK(ctx, launch_reduce_best(ctx->d_slots, n_warps, ctx->d_best, ctx->stream), "reduce kernel");
+  CK(ctx, cudaMemcpyAsync(ctx->h_best, ctx->d_best, sizeof(BestSlot), cudaMemcpyDeviceToHost, ctx->stream),
+     "read result");
+  CK(ctx, cudaStreamSynchronize(ctx->stream), "scan");
+  *best_out = *ctx->h_best;
+  if (top_k > 1) {
+    std::vector<BestSlot> cand((size_t)n_warps * 32);
+    CK(ctx, cudaMemcpy(cand.data(), ctx->d_cand, cand.size() * sizeof(BestSlot), cudaMemcpyDeviceToHost),
+       "read candidates");
+    std::sort(cand.begin(), cand.end(), [](const BestSlot& a, const BestSlot& b) {
+      return a.score < b.score || (a.score == b.score && a.key < b.key);
+    });
+    ctx->last_topk.clear();
+    for (const BestSlot& c : cand) {
+      if ((int)ctx->last_topk.size() >= top_k || c.key == ~0ull) break;
+      epik2_best e{};
+      e.score = c.score;
+      e.score_fp64 = std::numeric_limits<double>::quiet_NaN();
+      decode_key(c.key, e.i, e.j, e.k);
+      ctx->last_topk.push_back(e);
+    }
+  }
+  return EPIK2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* epik2_strerror(int status) {
+  switch (status) {
+    case EPIK2_OK: return "ok";
+    case EPIK2_E_INVALID: return "invalid argument";
+    case EPIK2_E_CUDA: return "CUDA error";
+    case EPIK2_E_NOMEM: return "out of device memory";
+    case EPIK2_E_NOT_FOUND: return "not found";
+    case EPIK2_E_TOO_LARGE: return "size beyond limit";
+    case EPIK2_E_TIMEOUT: return "timeout";
+    case EPIK2_E_NO_DEVICE: return "no suitable CUDA device";
+    case EPIK2_E_BUSY: return "busy";
+    case EPIK2_E_CANCELLED: return "cancelled";
+    default: return "unknown status";
+  }
+}
+
+const char* epik2_last_error(const epik2_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int epik2_create(epik2_ctx** out, int device) {
+  if (!out) return EPIK2_E_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return EPIK2_E_NO_DEVICE;
+  if (device < 0 || device >= n) return EPIK2_E_INVALID;
+  std::unique_ptr<epik2_ctx> ctx(new epik2_ctx());
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) return EPIK2_E_NO_DEVICE;
+  if (cudaGetDeviceProperties(&ctx->prop, device) != cudaSuccess) return EPIK2_E_NO_DEVICE;
+  if (ctx->prop.major != 10) return EPIK2_E_NO_DEVICE;  // built for sm_100a only
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return EPIK2_E_CUDA;
+  ctx->scan_blocks = ctx->prop.multiProcessorCount * scan_blocks_per_sm();
+  const int n_warps = ctx->scan_blocks * (kScanThreads / 32);
+  if (cudaMalloc(&ctx->d_counter, 64) != cudaSuccess || cudaMalloc(&ctx->d_slots, sizeof(BestSlot) * n_warps) ||
+      cudaMalloc(&ctx->d_best, sizeof(BestSlot)) || cudaMalloc(&ctx->d_cand, sizeof(BestSlot) * n_warps * 32) ||
+      cudaMallocHost(&ctx->h_best, sizeof(BestSlot))) {
+    epik2_destroy(ctx.release());
+    return EPIK2_E_NOMEM;
+  }
+  *out = ctx.release();
+  return EPIK2_OK;
+}
+
+void epik2_destroy(epik2_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->datasets) cudaFree(kv.second->block);
+  ctx->datasets.clear();
+  cudaFree(ctx->d_counter);
+  cudaFree(ctx->d_slots);
+  cudaFree(ctx->d_best);
+  cudaFree(ctx->d_cand);
+  cudaFree(ctx->d_pgoff);
+  cudaFreeHost(ctx->h_best);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int epik2_device_name(const epik2_ctx* ctx, char* buf, size_t len) {
+  if (!ctx || !buf || len == 0) return EPIK2_E_INVALID;
+  snprintf(buf, len, "%s", ctx->prop.name);
+  return EPIK2_OK;
+}
+
+int epik2_mem_info(const epik2_ctx* ctx, size_t* free_bytes, size_t* total_bytes) {
+  if (!ctx || !free_bytes || !total_bytes) return EPIK2_E_INVALID;
+  cudaSetDevice(ctx->device);
+  return cudaMemGetInfo(free_bytes, total_bytes) == cudaSuccess ? EPIK2_OK : EPIK2_E_CUDA;
+}
+
+int epik2_generate_reference(int64_t n_samples, int64_t n_snps, uint8_t* geno, uint8_t* pheno) {
+  if (n_samples < 1 || n_snps < 1 || !geno || !pheno || n_samples > INT32_MAX) return EPIK2_E_INVALID;
+  generate_reference(n_samples, n_snps, geno, pheno);
+  return EPIK2_OK;
+}
+
+int epik2_generate_hwe(uint64_t seed, int64_t n_samples, int64_t n_snps, int64_t n_cases, double maf_lo,
+                       double maf_hi, int32_t n_planted, const int64_t* planted, const double* effects, uint8_t* geno,
+                       uint8_t* pheno) {
+  if (n_samples < 1 || n_snps < 1 || !geno || !pheno || n_cases < 0 || n_cases > n_samples) return EPIK2_E_INVALID;
+  if (!(maf_lo >= 0.0 && maf_hi <= 1.0 && maf_lo <= maf_hi)) return EPIK2_E_INVALID;
+  if (n_planted < 0 || (n_planted > 0 && (!planted || !effects))) return EPIK2_E_INVALID;
+  for (int t = 0; t < n_planted; t++) {
+    for (int q = 0; q < 3; q++)
+      if (planted[3 * t + q] < 0 || planted[3 * t + q] >= n_snps) return EPIK2_E_INVALID;
+    if (!(effects[t] > 0.0 && effects[t] < 1.0)) return EPIK2_E_INVALID;
+  }
+  generate_hwe(seed, n_samples, n_snps, n_cases, maf_lo, maf_hi, n_planted, planted, effects, geno, pheno);
+  return EPIK2_OK;
+}
+
+int64_t epik2_dataset_bytes(int64_t n_samples, int64_t n_snps) {
+  if (n_samples < 1 || n_snps < 1) return -1;
+  return (int64_t)dataset_layout(n_samples, n_snps).total;
+}
+
+int epik2_load_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int64_t n_samples, int64_t n_snps,
+                  int32_t* dataset_id) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (!geno || !pheno || !dataset_id) return fail(ctx, EPIK2_E_INVALID, "null pointer");
+  if (n_samples < 1 || n_snps < 1) return fail(ctx, EPIK2_E_INVALID, "n_samples and n_snps must be >= 1");
+  if (n_samples > EPIK2_MAX_SAMPLES || n_snps > EPIK2_MAX_SNPS)
+    return fail(ctx, EPIK2_E_TOO_LARGE, "n_samples or n_snps beyond limit");
+  CK(ctx, cudaSetDevice(ctx->device), "set device");
+  const Layout L = dataset_layout(n_samples, n_snps);
+  size_t fr = 0, tot = 0;
+  CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
+  if (L.total + (size_t)(256u << 20) > fr) return fail(ctx, EPIK2_E_NOMEM, "dataset does not fit in free device memory");
+  std::unique_ptr<DevDataset> d(new DevDataset());
+  CK(ctx, cudaMalloc(&d->block, L.total), "alloc dataset");
+  char* b = (char*)d->block;
+  d->bytes = L.total;
+  d->n_samples = n_samples;
+  d->n_snps = n_snps;
+  d->m_pad = (n_snps + 31) / 32 * 32;
+  d->tri = tri_size(d->m_pad);
+  d->geno = (uint8_t*)(b + L.geno);
+  d->perm = (int32_t*)(b + L.perm);
+  d->planes = (uint2*)(b + L.planes);
+  d->singles = (uint32_t*)(b + L.singles);
+  d->pairs = (uint4*)(b + L.pairs);
+  d->lut = (float*)(b + L.lut);
+  std::vector<float> lut((size_t)n_samples + 2);
+  build_k2_lut(n_samples + 1, lut.data());
+  cudaError_t e = cudaMemcpyAsync(d->geno, geno, (size_t)(n_samples * n_snps), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d->lut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaFree(d->block);
+    return cuda_fail(ctx, e, "upload dataset");
+  }
+  int r = encode_with(ctx, *d, pheno);
+  if (r) {
+    cudaFree(d->block);
+    return r;
+  }
+  const int32_t id = ctx->next_id++;
+  ctx->datasets[id] = std::move(d);
+  *dataset_id = id;
+  return EPIK2_OK;
+}
+
+int epik2_set_pheno(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* pheno) {
+  if (!ctx) return EPIK2_E_INVALID;
+  DevDataset* d = find(ctx, dataset_id);
+  if (!d) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
+  if (!pheno) return fail(ctx, EPIK2_E_INVALID, "null phenotype");
+  CK(ctx, cudaSetDevice(ctx->device), "set device");
+  return encode_with(ctx, *d, pheno);
+}
+
+int epik2_unload(epik2_ctx* ctx, int32_t dataset_id) {
+  if (!ctx) return EPIK2_E_INVALID;
+  auto it = ctx->datasets.find(dataset_id);
+  if (it == ctx->datasets.end()) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(it->second->block);
+  ctx->datasets.erase(it);
+  return EPIK2_OK;
+}
+
+int epik2_dataset_info(const epik2_ctx* ctx, int32_t dataset_id, int64_t* n_samples, int64_t* n_snps,
+                       int64_t* n_cases, int64_t* device_bytes) {
+  if (!ctx) return EPIK2_E_INVALID;
+  auto it = ctx->datasets.find(dataset_id);
+  if (it == ctx->datasets.end()) return EPIK2_E_NOT_FOUND;
+  const DevDataset& d = *it->second;
+  if (n_samples) *n_samples = d.n_samples;
+  if (n_snps) *n_snps = d.n_snps;
+  if (n_cases) *n_cases = d.n_cases;
+  if (device_bytes) *device_bytes = (int64_t)d.bytes;
+  return EPIK2_OK;
+}
+
+int epik2_scan(epik2_ctx* ctx, int32_t dataset_id, const epik2_opts* opts, epik2_best* out) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (!out) return fail(ctx, EPIK2_E_INVALID, "null output");
+  DevDataset* d = find(ctx, dataset_id);
+  if (!d) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
+  if (d->n_snps < 3) return fail(ctx, EPIK2_E_INVALID, "need at least 3 SNPs");
+  CK(ctx, cudaSetDevice(ctx->device), "set device");
+  BestSlot b{};
+  int r = run_scan(ctx, *d, opts, nullptr, nullptr, &b);
+  if (r) return r;
+  out->score = b.score;
+  out->score_fp64 = std::numeric_limits<double>::quiet_NaN();
+  decode_key(b.key, out->i, out->j, out->k);
+  if (b.key == ~0ull) return fail(ctx, EPIK2_E_INVALID, "no triplet in the requested range");
+  return EPIK2_OK;
+}
+
+int epik2_scan_topk(epik2_ctx* ctx, int32_t dataset_id, const epik2_opts* opts, epik2_best* out, int32_t capacity,
+                    int32_t* n_out) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (!out || !n_out || capacity < 1) return fail(ctx, EPIK2_E_INVALID, "bad output buffer");
+  epik2_opts o{};
+  if (opts) o = *opts;
+  if (o.top_k < 2) o.top_k = std::min(capacity, 32);
+  epik2_best best{};
+  int r = epik2_scan(ctx, dataset_id, &o, &best);
+  if (r) return r;
+  const int n = std::min<int>(capacity, (int)ctx->last_topk.size());
+  for (int t = 0; t < n; t++) out[t] = ctx->last_topk[(size_t)t];
+  *n_out = n;
+  return EPIK2_OK;
+}
+
+int epik2_scan_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int64_t n_samples, int64_t n_snps,
+                  const epik2_opts* opts, epik2_best* out) {
+  int32_t id = 0;
+  int r = epik2_load_u8(ctx, geno, pheno, n_samples, n_snps, &id);
+  if (r) return r;
+  r = epik2_scan(ctx, id, opts, out);
+  epik2_unload(ctx, id);
+  return r;
+}
+
+int epik2_dump_tables(epik2_ctx* ctx, int32_t dataset_id, uint32_t* tables, float* scores) {
+  if (!ctx) return EPIK2_E_INVALID;
+  DevDataset* d = find(ctx, dataset_id);
+  if (!d) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
+  const int64_t m = d->n_snps;
+  if (m < 3) return fail(ctx, EPIK2_E_INVALID, "need at least 3 SNPs");
+  if (m > 512) return fail(ctx, EPIK2_E_TOO_LARGE, "dump limited to 512 SNPs");
+  CK(ctx, cudaSetDevice(ctx->device), "set device");
+  const int64_t T = m * (m - 1) * (m - 2) / 6;
+  uint32_t* dt = nullptr;
+  float* ds = nullptr;
+  CK(ctx, cudaMalloc(&dt, (size_t)T * 54 * 4), "alloc dump");
+  cudaError_t e = cudaMalloc(&ds, (size_t)T * 4);
+  if (e != cudaSuccess) {
+    cudaFree(dt);
+    return cuda_fail(ctx, e, "alloc dump");
+  }
+  BestSlot b{};
+  int r = run_scan(ctx, *d, nullptr, dt, ds, &b);
+  if (r == EPIK2_OK) {
+    e = cudaSuccess;
+    if (tables) e = cudaMemcpy(tables, dt, (size_t)T * 54 * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && scores) e = cudaMemcpy(scores, ds, (size_t)T * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) r = cuda_fail(ctx, e, "read dump");
+  }
+  cudaFree(dt);
+  cudaFree(ds);
+  return r;
+}
+
+int epik2_tables(epik2_ctx* ctx, int32_t dataset_id, const uint32_t* triplets, int64_t n, uint32_t* tables) {
+  if (!ctx) return EPIK2_E_INVALID;
+  DevDataset* d = find(ctx, dataset_id);
+  if (!d) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
+  if (n < 0 || (n > 0 && (!triplets || !tables))) return fail(ctx, EPIK2_E_INVALID, "bad triplet list");
+  if (n == 0) return EPIK2_OK;
+  for (int64_t t = 0; t < n; t++) {
+    const uint32_t i = triplets[3 * t], j = triplets[3 * t + 1], k = triplets[3 * t + 2];
+    if (!(i < j && j < k && (int64_t)k < d->n_snps)) return fail(ctx, EPIK2_E_INVALID, "triplet out of range");
+  }
+  CK(ctx, cudaSetDevice(ctx->device), "set device");
+  uint32_t *dtrip = nullptr, *dout = nullptr;
+  CK(ctx, cudaMalloc(&dtrip, (size_t)n * 12), "alloc triplets");
+  cudaError_t e = cudaMalloc(&dout, (size_t)n * 54 * 4);
+  if (e == cudaSuccess) e = cudaMemcpy(dtrip, triplets, (size_t)n * 12, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_tables(*d, dtrip, n, dout, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(tables, dout, (size_t)n * 54 * 4, cudaMemcpyDeviceToHost);
+  cudaFree(dtrip);
+  cudaFree(dout);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tables");
+  return EPIK2_OK;
+}
+
+int epik2_k2_lut(int64_t n_max, float* lut) {
+  if (n_max < 0 || !lut) return EPIK2_E_INVALID;
+  build_k2_lut(n_max, lut);
+  return EPIK2_OK;
+}
+
+}  // extern "C"

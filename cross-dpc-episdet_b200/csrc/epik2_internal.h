@@ -1,0 +1,83 @@
+// Internal declarations shared by the host API and the CUDA kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace epik2 {
+
+constexpr int kWarp = 32;
+constexpr int kPairsPerWarp = 4;      // (i, j0..j0+3) pair group handled by one warp
+constexpr int kScanThreads = 256;     // 8 warps per CTA
+constexpr int kTableMaxSize = 748;    // reference TABLE_MAX_SIZE (GPU/v4.cpp:15)
+
+// Device-resident dataset.  Planes are word-major: for each 32-sample class word w
+// (controls' words first, then cases'), one uint2 {g0 bits, g1 bits} per SNP, rows of
+// m_pad SNPs.  Bit b of class word w is the sample of rank 32*w' + b in its class
+// (w' = word index inside the class); padding bits and padding SNPs are zero.
+struct DevDataset {
+  int64_t n_samples = 0, n_snps = 0, n_cases = 0, n_controls = 0;
+  int64_t m_pad = 0;      // n_snps rounded up to 32
+  int64_t w0 = 0, w1 = 0; // words per class
+  uint8_t* geno = nullptr;      // [n_samples][n_snps], kept for phenotype re-encoding
+  int32_t* perm = nullptr;      // class-sorted sample order: controls then cases
+  uint2* planes = nullptr;      // [w0+w1][m_pad]
+  uint32_t* singles = nullptr;  // [2][m_pad][2] counts of g0, g1 per class
+  uint4* pairs = nullptr;       // [2][tri(m_pad)] counts (00,01,10,11) for x<y
+  float* lut = nullptr;         // ln n! in the reference CPU arithmetic, [0, n_samples+1]
+  int64_t tri = 0;              // entries per class in `pairs`
+  void* block = nullptr;        // single allocation holding all of the above
+  size_t bytes = 0;
+};
+
+// Offset of pair (x, y), x < y, in a row-major strict upper triangle of an m x m matrix.
+__host__ __device__ inline int64_t tri_offset(int64_t m, int64_t x, int64_t y) {
+  return x * (m - 1) - (x * (x - 1)) / 2 + (y - x - 1);
+}
+__host__ __device__ inline int64_t tri_size(int64_t m) { return m * (m - 1) / 2; }
+
+// Best-candidate record: score (positive float) + packed lexicographic key.
+struct BestSlot {
+  float score;
+  uint32_t pad;
+  unsigned long long key;  // (i << 42) | (j << 21) | k
+};
+
+__host__ __device__ inline unsigned long long pack_key(uint64_t i, uint64_t j, uint64_t k) {
+  return (i << 42) | (j << 21) | k;
+}
+
+struct ScanParams {
+  const uint2* planes;
+  const uint32_t* singles;
+  const uint4* pairs;
+  const float* lut;
+  const int64_t* pg_off;   // prefix sums of pair groups per first index, [n_first + 1]
+  int64_t n_groups;
+  int64_t tri;
+  int32_t n_first;         // number of first indices covered
+  int32_t i_begin;
+  int32_t m, m_pad, w0, w1, n0, n1;
+  unsigned long long* counter;
+  BestSlot* slots;         // one per warp in the grid
+  int32_t top_k;           // >1: per-warp candidate lists of this many entries
+  BestSlot* cand;          // [warps][top_k] when top_k > 1
+  uint32_t* dump_tables;   // [C(m,3)][54] or null
+  float* dump_scores;      // [C(m,3)] or null
+};
+
+// Kernel launchers (scan_int.cu / encode.cu); all asynchronous on `stream`.
+cudaError_t launch_encode(const DevDataset& d, cudaStream_t stream);
+cudaError_t launch_counts(const DevDataset& d, cudaStream_t stream);
+cudaError_t launch_scan_int(const ScanParams& p, int blocks, bool dump, cudaStream_t stream);
+cudaError_t launch_reduce_best(const BestSlot* slots, int n, BestSlot* out, cudaStream_t stream);
+cudaError_t launch_tables(const DevDataset& d, const uint32_t* triplets, int64_t n, uint32_t* out,
+                          cudaStream_t stream);
+int scan_blocks_per_sm();
+
+// Host helpers (host_data.cpp).
+void build_k2_lut(int64_t n_max, float* lut);
+void generate_reference(int64_t n, int64_t m, uint8_t* geno, uint8_t* pheno);
+void generate_hwe(uint64_t seed, int64_t n, int64_t m, int64_t n_cases, double maf_lo, double maf_hi,
+                  int n_planted, const int64_t* planted, const double* effects, uint8_t* geno, uint8_t* pheno);
+
+}  // namespace epik2

@@ -1,0 +1,268 @@
+"""Python host binding of libepik2 (the C ABI in include/epik2.h).
+
+The compute path is the CUDA library; this module only marshals arguments.  There is
+no CPU fallback: if the shared library is missing or no sm_100 GPU is visible, the
+calls raise.
+"""
+import ctypes
+import math
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(HERE)
+REPO_ROOT = os.path.dirname(PKG_ROOT)
+LIB_PATH = os.path.join(HERE, "lib", "libepik2.so")
+CLI_PATH = os.path.join(HERE, "bin", "epik2_v4")
+HEADER = os.path.join(REPO_ROOT, "include", "epik2.h")
+
+OK = 0
+E_INVALID = -1
+E_CUDA = -2
+E_NOMEM = -3
+E_NOT_FOUND = -4
+E_TOO_LARGE = -5
+E_TIMEOUT = -6
+E_NO_DEVICE = -7
+E_BUSY = -8
+E_CANCELLED = -9
+
+
+class Epik2Error(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"epik2 status {status}: {msg}")
+        self.status = status
+
+
+class Best(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_float), ("_pad", ctypes.c_float), ("score_fp64", ctypes.c_double),
+                ("i", ctypes.c_uint32), ("j", ctypes.c_uint32), ("k", ctypes.c_uint32), ("_pad2", ctypes.c_uint32)]
+
+    @property
+    def ijk(self):
+        return (int(self.i), int(self.j), int(self.k))
+
+    def __repr__(self):
+        return f"Best(score={self.score!r}, score_fp64={self.score_fp64!r}, ijk={self.ijk})"
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("engine", ctypes.c_int32), ("top_k", ctypes.c_int32), ("rescore_fp64", ctypes.c_int32),
+                ("k_strip", ctypes.c_int32), ("pairs_per_warp", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("snp_begin", ctypes.c_int64), ("snp_end", ctypes.c_int64)]
+
+
+_lib = None
+
+
+def exported_symbols():
+    """Function names declared in include/epik2.h."""
+    with open(HEADER) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(epik2_[a-z0-9_]+)\s*\(", text)))
+
+
+def library():
+    """Load libepik2.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise Epik2Error(E_NO_DEVICE, f"{LIB_PATH} not built (run __graft_entry__.build() or make -C {PKG_ROOT})")
+    L = ctypes.CDLL(LIB_PATH)
+    p, i32, i64, u64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64
+    sig = {
+        "epik2_create": ([ctypes.POINTER(p), ctypes.c_int], ctypes.c_int),
+        "epik2_destroy": ([p], None),
+        "epik2_strerror": ([ctypes.c_int], ctypes.c_char_p),
+        "epik2_last_error": ([p], ctypes.c_char_p),
+        "epik2_device_name": ([p, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+        "epik2_mem_info": ([p, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
+        "epik2_generate_reference": ([i64, i64, p, p], ctypes.c_int),
+        "epik2_generate_hwe": ([u64, i64, i64, i64, ctypes.c_double, ctypes.c_double, i32, p, p, p, p], ctypes.c_int),
+        "epik2_load_u8": ([p, p, p, i64, i64, ctypes.POINTER(i32)], ctypes.c_int),
+        "epik2_set_pheno": ([p, i32, p], ctypes.c_int),
+        "epik2_unload": ([p, i32], ctypes.c_int),
+        "epik2_dataset_info": ([p, i32, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64),
+                                ctypes.POINTER(i64)], ctypes.c_int),
+        "epik2_dataset_bytes": ([i64, i64], i64),
+        "epik2_scan": ([p, i32, ctypes.POINTER(Opts), ctypes.POINTER(Best)], ctypes.c_int),
+        "epik2_scan_topk": ([p, i32, ctypes.POINTER(Opts), ctypes.POINTER(Best), i32, ctypes.POINTER(i32)],
+                            ctypes.c_int),
+        "epik2_scan_u8": ([p, p, p, i64, i64, ctypes.POINTER(Opts), ctypes.POINTER(Best)], ctypes.c_int),
+        "epik2_dump_tables": ([p, i32, p, p], ctypes.c_int),
+        "epik2_tables": ([p, i32, p, i64, p], ctypes.c_int),
+        "epik2_k2_lut": ([i64, p], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def strerror(status):
+    return library().epik2_strerror(status).decode()
+
+
+def generate_reference(n_samples, n_snps):
+    """The reference's srand(100) synthetic data: (geno [S][M] uint8, pheno [S] uint8)."""
+    g = np.empty((n_samples, n_snps), dtype=np.uint8)
+    ph = np.empty(n_samples, dtype=np.uint8)
+    r = library().epik2_generate_reference(n_samples, n_snps, _ptr(g), _ptr(ph))
+    if r:
+        raise Epik2Error(r, strerror(r))
+    return g, ph
+
+
+def generate_hwe(seed, n_samples, n_snps, n_cases, maf=(0.05, 0.5), planted=(), effects=()):
+    """Seeded Hardy-Weinberg matrix with planted triplets: (geno [S][M] uint8, pheno [S] uint8)."""
+    g = np.empty((n_samples, n_snps), dtype=np.uint8)
+    ph = np.empty(n_samples, dtype=np.uint8)
+    pl = np.ascontiguousarray(np.array(planted, dtype=np.int64).reshape(-1, 3))
+    ef = np.ascontiguousarray(np.array(effects, dtype=np.float64).reshape(-1))
+    if len(pl) != len(ef):
+        raise ValueError("planted and effects differ in length")
+    r = library().epik2_generate_hwe(seed, n_samples, n_snps, n_cases, float(maf[0]), float(maf[1]), len(pl),
+                                     _ptr(pl), _ptr(ef), _ptr(g), _ptr(ph))
+    if r:
+        raise Epik2Error(r, strerror(r))
+    return g, ph
+
+
+def k2_lut(n_max):
+    out = np.empty(n_max + 1, dtype=np.float32)
+    r = library().epik2_k2_lut(n_max, _ptr(out))
+    if r:
+        raise Epik2Error(r, strerror(r))
+    return out
+
+
+def dataset_bytes(n_samples, n_snps):
+    return int(library().epik2_dataset_bytes(n_samples, n_snps))
+
+
+def n_triplets(m):
+    return m * (m - 1) * (m - 2) // 6 if m >= 3 else 0
+
+
+class Context:
+    """One device context: owns a CUDA stream and the resident datasets."""
+
+    def __init__(self, device=0):
+        self._lib = library()
+        h = ctypes.c_void_p()
+        r = self._lib.epik2_create(ctypes.byref(h), device)
+        if r:
+            raise Epik2Error(r, strerror(r))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.epik2_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, r):
+        if r:
+            msg = self._lib.epik2_last_error(self._h)
+            raise Epik2Error(r, f"{strerror(r)}: {msg.decode() if msg else ''}")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_name(self):
+        buf = ctypes.create_string_buffer(256)
+        self._check(self._lib.epik2_device_name(self._h, buf, 256))
+        return buf.value.decode()
+
+    def mem_info(self):
+        fr, tot = ctypes.c_size_t(), ctypes.c_size_t()
+        self._check(self._lib.epik2_mem_info(self._h, ctypes.byref(fr), ctypes.byref(tot)))
+        return fr.value, tot.value
+
+    def load(self, geno, pheno):
+        geno = np.ascontiguousarray(geno, dtype=np.uint8)
+        pheno = np.ascontiguousarray(pheno, dtype=np.uint8)
+        if geno.ndim != 2 or pheno.shape != (geno.shape[0],):
+            raise ValueError("geno must be [n_samples][n_snps] and pheno [n_samples]")
+        did = ctypes.c_int32()
+        self._check(self._lib.epik2_load_u8(self._h, _ptr(geno), _ptr(pheno), geno.shape[0], geno.shape[1],
+                                            ctypes.byref(did)))
+        return did.value
+
+    def set_pheno(self, dataset, pheno):
+        pheno = np.ascontiguousarray(pheno, dtype=np.uint8)
+        self._check(self._lib.epik2_set_pheno(self._h, dataset, _ptr(pheno)))
+
+    def unload(self, dataset):
+        self._check(self._lib.epik2_unload(self._h, dataset))
+
+    def info(self, dataset):
+        s, m, c, b = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(self._lib.epik2_dataset_info(self._h, dataset, ctypes.byref(s), ctypes.byref(m), ctypes.byref(c),
+                                                 ctypes.byref(b)))
+        return {"n_samples": s.value, "n_snps": m.value, "n_cases": c.value, "device_bytes": b.value}
+
+    @staticmethod
+    def _opts(**kw):
+        o = Opts()
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+    def scan(self, dataset, **opts):
+        o = self._opts(**opts)
+        b = Best()
+        self._check(self._lib.epik2_scan(self._h, dataset, ctypes.byref(o), ctypes.byref(b)))
+        return b
+
+    def scan_topk(self, dataset, k=32, **opts):
+        o = self._opts(top_k=k, **opts)
+        arr = (Best * k)()
+        n = ctypes.c_int32()
+        self._check(self._lib.epik2_scan_topk(self._h, dataset, ctypes.byref(o), arr, k, ctypes.byref(n)))
+        return [arr[t] for t in range(n.value)]
+
+    def scan_u8(self, geno, pheno, **opts):
+        geno = np.ascontiguousarray(geno, dtype=np.uint8)
+        pheno = np.ascontiguousarray(pheno, dtype=np.uint8)
+        o = self._opts(**opts)
+        b = Best()
+        self._check(self._lib.epik2_scan_u8(self._h, _ptr(geno), _ptr(pheno), geno.shape[0], geno.shape[1],
+                                            ctypes.byref(o), ctypes.byref(b)))
+        return b
+
+    def dump_tables(self, dataset):
+        m = self.info(dataset)["n_snps"]
+        T = n_triplets(m)
+        tables = np.zeros((T, 54), dtype=np.uint32)
+        scores = np.zeros(T, dtype=np.float32)
+        self._check(self._lib.epik2_dump_tables(self._h, dataset, _ptr(tables), _ptr(scores)))
+        return tables, scores
+
+    def tables(self, dataset, triplets):
+        t = np.ascontiguousarray(np.asarray(triplets, dtype=np.uint32).reshape(-1, 3))
+        out = np.zeros((len(t), 54), dtype=np.uint32)
+        self._check(self._lib.epik2_tables(self._h, dataset, _ptr(t), len(t), _ptr(out)))
+        return out

@@ -1,0 +1,153 @@
+/*
+ * epik2.h -- C ABI of the B200 exhaustive third-order K2 epistasis search.
+ *
+ * Drop-in for the GPU search path of hiperbio/cross-dpc-episdet (GPU/v1.cpp-v4.cpp).
+ * The reference has no library interface: its seams are the process CLI
+ * (GPU/v4.cpp:210-212, 610-612) and, inside main(), the hand-off from encoding to the
+ * search kernel (GPU/v4.cpp:219-297) and from the kernel to the host argmin
+ * (GPU/v4.cpp:599-608).  Each entry point below names the reference code it replaces.
+ *
+ * Conventions
+ *   - Every function returns 0 (EPIK2_OK) or a negative EPIK2_E_* status; no exception
+ *     or longjmp crosses the ABI.  epik2_last_error() gives the message of the last
+ *     failure on a context.
+ *   - The caller owns every host buffer; the library owns every device buffer through
+ *     the context and frees it in epik2_unload / epik2_destroy.
+ *   - A context belongs to one host thread at a time (the serving loop in this library
+ *     serialises its own use).
+ *   - Genotypes are uint8 in {0,1,2}, sample-major [n_samples][n_snps], the layout of the
+ *     reference's generate_data (GPU/v4.cpp:94).  As in the reference's encoder
+ *     (GPU/v4.cpp:161-171) any value other than 0 or 1 counts as genotype 2.
+ *   - Phenotype is uint8 [n_samples]; value 1 = case, anything else = control
+ *     (GPU/v4.cpp:152).
+ *   - Triplets are 0-based SNP indices i < j < k.  Ties in score go to the lowest
+ *     (i, j, k) in lexicographic order.
+ *   - Contingency tables are 54 uint32: cell c = 9*g_i + 3*g_j + g_k, controls in
+ *     [0,27), cases in [27,54) (GPU/v4.cpp:317-319).
+ */
+#ifndef EPIK2_H
+#define EPIK2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EPIK2_ABI_VERSION 1
+
+/* status codes */
+#define EPIK2_OK 0
+#define EPIK2_E_INVALID (-1)   /* bad argument (null pointer, size out of range, unknown option) */
+#define EPIK2_E_CUDA (-2)      /* CUDA runtime error; the context stays usable unless noted */
+#define EPIK2_E_NOMEM (-3)     /* device memory exhausted, or admission refused for lack of HBM */
+#define EPIK2_E_NOT_FOUND (-4) /* unknown dataset or request handle */
+#define EPIK2_E_TOO_LARGE (-5) /* size beyond a documented limit */
+#define EPIK2_E_TIMEOUT (-6)   /* a bounded device-side or host-side wait expired */
+#define EPIK2_E_NO_DEVICE (-7) /* no CUDA device, or not an sm_100 device */
+#define EPIK2_E_BUSY (-8)      /* request still running (epik2_poll) */
+#define EPIK2_E_CANCELLED (-9) /* request cancelled before it ran */
+
+/* limits */
+#define EPIK2_MAX_SNPS (1 << 20)      /* i, j, k packed in 21 bits each for the argmin key */
+#define EPIK2_MAX_SAMPLES (1 << 26)   /* counts and LUT index fit in 32 bits with margin */
+#define EPIK2_MAX_TOPK 256
+
+typedef struct epik2_ctx epik2_ctx;
+
+/* Best triplet.  `score` is the K2 score in the reference CPU path's FP32 arithmetic
+ * (CPU/v2.cpp:514-517); `score_fp64` is the same triplet rescored in FP64 on the GPU
+ * (precision form) or NaN when not requested. */
+typedef struct {
+  float score;
+  float _pad;
+  double score_fp64;
+  uint32_t i, j, k;
+  uint32_t _pad2;
+} epik2_best;
+
+/* Scan options.  Zero-initialise and set what you need; 0 means "default". */
+typedef struct {
+  int32_t engine;      /* 0 = default (fastest available), 1 = integer-pipe kernel */
+  int32_t top_k;       /* 0/1 = best only; >1 = keep the top_k lowest FP32 scores */
+  int32_t rescore_fp64;/* 1 = rescore the kept candidates in FP64 on the GPU */
+  int32_t k_strip;     /* tuning: SNPs per k-strip (multiple of 32); 0 = autotuned */
+  int32_t pairs_per_warp; /* tuning: reserved, 0 = default */
+  int32_t blocks_per_sm;  /* tuning: 0 = occupancy-derived */
+  int64_t snp_begin;   /* restrict the first index i to [snp_begin, snp_end); 0,0 = all */
+  int64_t snp_end;
+} epik2_opts;
+
+/* --------------------------------------------------------------------------------
+ * Context.  Replaces the SYCL queue/device selection of GPU/v4.cpp:243-251.
+ * ------------------------------------------------------------------------------ */
+int epik2_create(epik2_ctx **out, int device);
+void epik2_destroy(epik2_ctx *ctx);
+const char *epik2_strerror(int status);
+const char *epik2_last_error(const epik2_ctx *ctx);
+/* Device name as the reference prints it ("Selected device: ...", GPU/v4.cpp:251). */
+int epik2_device_name(const epik2_ctx *ctx, char *buf, size_t len);
+/* Bytes of device memory currently free / total on the context's device. */
+int epik2_mem_info(const epik2_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
+
+/* --------------------------------------------------------------------------------
+ * Data sources (host).  The reference synthesises its input inside main().
+ * ------------------------------------------------------------------------------ */
+/* The reference's generator: srand(100), geno[s][m] = rand()%3, exactly n/2 cases by
+ * rejection sampling (GPU/v4.cpp:81-110).  pheno must hold n_samples bytes. */
+int epik2_generate_reference(int64_t n_samples, int64_t n_snps, uint8_t *geno, uint8_t *pheno);
+/* Seeded Hardy-Weinberg generator with planted triplets (benchmark workloads; no
+ * reference counterpart).  planted = n_planted*3 SNP indices, effects = case
+ * probability for carriers of each planted triplet. */
+int epik2_generate_hwe(uint64_t seed, int64_t n_samples, int64_t n_snps, int64_t n_cases, double maf_lo,
+                       double maf_hi, int32_t n_planted, const int64_t *planted, const double *effects,
+                       uint8_t *geno, uint8_t *pheno);
+
+/* --------------------------------------------------------------------------------
+ * Datasets.  Replaces data_to_binary + binary_to_tiled + masks + the USM uploads
+ * (GPU/v4.cpp:112-196, 220-238, 256-262): uploads the matrix, encodes per-class bit
+ * planes on the GPU and keeps them resident until epik2_unload.
+ * ------------------------------------------------------------------------------ */
+int epik2_load_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int64_t n_samples,
+                  int64_t n_snps, int32_t *dataset_id);
+/* Re-encode a resident dataset with a new phenotype vector (permutation replicate). */
+int epik2_set_pheno(epik2_ctx *ctx, int32_t dataset_id, const uint8_t *pheno);
+int epik2_unload(epik2_ctx *ctx, int32_t dataset_id);
+/* n_samples, n_snps, n_cases, and device bytes held by the dataset. */
+int epik2_dataset_info(const epik2_ctx *ctx, int32_t dataset_id, int64_t *n_samples, int64_t *n_snps,
+                       int64_t *n_cases, int64_t *device_bytes);
+/* Device bytes a dataset of this shape would hold (admission control). */
+int64_t epik2_dataset_bytes(int64_t n_samples, int64_t n_snps);
+
+/* --------------------------------------------------------------------------------
+ * Search.  Replaces the host tile loop + kernel_epi + host argmin
+ * (GPU/v4.cpp:283-608; same result as GPU/v2.cpp:260-565 with its lexicographic
+ * tie-break).
+ * ------------------------------------------------------------------------------ */
+int epik2_scan(epik2_ctx *ctx, int32_t dataset_id, const epik2_opts *opts, epik2_best *out);
+/* Top-k form: after a scan with opts->top_k = K, copy the K best (ascending FP32 score,
+ * ties by index) into out[0..K).  *n_out receives the number written. */
+int epik2_scan_topk(epik2_ctx *ctx, int32_t dataset_id, const epik2_opts *opts, epik2_best *out,
+                    int32_t capacity, int32_t *n_out);
+/* One call from host buffers to the best triplet: load + scan + unload. */
+int epik2_scan_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int64_t n_samples,
+                  int64_t n_snps, const epik2_opts *opts, epik2_best *out);
+
+/* --------------------------------------------------------------------------------
+ * Parity / inspection.  The reference keeps tables in registers (GPU/v4.cpp:317);
+ * these expose the same counts and scores computed by the search kernel itself.
+ * ------------------------------------------------------------------------------ */
+/* Every triplet's 54 counts and FP32 score, at its lexicographic index
+ * t(i,j,k) among the C(n_snps,3) triplets.  tables: C(M,3)*54 uint32 (may be NULL),
+ * scores: C(M,3) float (may be NULL).  Limited to n_snps <= 512. */
+int epik2_dump_tables(epik2_ctx *ctx, int32_t dataset_id, uint32_t *tables, float *scores);
+/* Tables of an explicit list of triplets (n x 3 SNP indices). */
+int epik2_tables(epik2_ctx *ctx, int32_t dataset_id, const uint32_t *triplets, int64_t n, uint32_t *tables);
+/* The FP32 log-factorial lookup table used by the score, lut[0..n_max]. */
+int epik2_k2_lut(int64_t n_max, float *lut);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EPIK2_H */

@@ -1,0 +1,89 @@
+import ctypes
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, os.path.join(ROOT, "cross-dpc-episdet_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs an sm_100 (B200) GPU; runs the CUDA path")
+    config.addinivalue_line("markers", "slow: takes more than a few seconds")
+
+
+def cuda_device_count():
+    for name in ("libcudart.so", "libcudart.so.12"):
+        try:
+            rt = ctypes.CDLL(name)
+            break
+        except OSError:
+            rt = None
+    if rt is None:
+        try:
+            import torch  # the venv's torch ships a cudart
+            return torch.cuda.device_count()
+        except Exception:
+            return 0
+    n = ctypes.c_int(0)
+    if rt.cudaGetDeviceCount(ctypes.byref(n)) != 0:
+        return 0
+    return n.value
+
+
+HAS_GPU = None
+
+
+def has_gpu():
+    global HAS_GPU
+    if HAS_GPU is None:
+        HAS_GPU = cuda_device_count() > 0
+    return HAS_GPU
+
+
+def pytest_collection_modifyitems(config, items):
+    if has_gpu():
+        return
+    skip = pytest.mark.skip(reason="no CUDA device in this container")
+    for item in items:
+        if "gpu" in item.keywords:
+            item.add_marker(skip)
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    import epik2
+    c = epik2.Context(0)
+    yield c
+    c.close()
+
+
+def load_tap(name):
+    z = np.load(os.path.join(GOLDEN, f"tap_{name}.npz"))
+    return {k: z[k] for k in z.files}
+
+
+TAP_CASES = ["refgen_256x20", "hwe_300x24_37cases", "hwe_40x12_5cases", "hwe_64x3", "hwe_1000x30_planted",
+             "odd_values_100x10"]
+
+
+def ref_kat():
+    return json.load(open(os.path.join(GOLDEN, "ref_kat.json")))
+
+
+def ref_best():
+    return json.load(open(os.path.join(GOLDEN, "ref_best.json")))
+
+
+def addlog_bits():
+    return np.load(os.path.join(GOLDEN, "addlog.npz"))["bits"]
+
+
+def f32_bits(x):
+    return int(np.array([x], dtype=np.float32).view(np.uint32)[0])
