@@ -17,7 +17,10 @@ using namespace epik2;
 
 struct epik2_ctx {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // current stream (own or caller's)
+  cudaStream_t own_stream = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  epik2_stats stats{};
   cudaDeviceProp prop{};
   std::string last_error;
   std::map<int32_t, std::unique_ptr<DevDataset>> datasets;
@@ -101,8 +104,10 @@ int encode_with(epik2_ctx* ctx, DevDataset& d, const uint8_t* pheno) {
   d.w0 = (d.n_controls + 31) / 32;
   d.w1 = (d.n_cases + 31) / 32;
   CK(ctx, cudaMemcpyAsync(d.perm, perm.data(), perm.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "upload perm");
+  ctx->stats.h2d_bytes += perm.size() * 4;
   CK(ctx, launch_encode(d, ctx->stream), "encode kernel");
   CK(ctx, launch_counts(d, ctx->stream), "count kernels");
+  ctx->stats.kernel_launches += 3;
   CK(ctx, cudaStreamSynchronize(ctx->stream), "encode");
   return EPIK2_OK;
 }
@@ -153,6 +158,7 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   if (r) return r;
   CK(ctx, cudaMemcpyAsync(ctx->d_pgoff, off.data(), off.size() * 8, cudaMemcpyHostToDevice, ctx->stream),
      "upload pair-group offsets");
+  ctx->stats.h2d_bytes += off.size() * 8;
   CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream), "reset counter");
   ScanParams p{};
   p.planes = d.planes;
@@ -177,17 +183,34 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   p.dump_tables = dump_tables;
   p.dump_scores = dump_scores;
   const bool dump = dump_tables != nullptr;
+  CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
   CK(ctx, launch_scan_int(p, ctx->scan_blocks, dump, ctx->stream), "scan kernel");
+  CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
   const int n_warps = ctx->scan_blocks * (kScanThreads / 32);
   CK(ctx, launch_reduce_best(ctx->d_slots, n_warps, ctx->d_best, ctx->stream), "reduce kernel");
+  ctx->stats.kernel_launches += 2;
   CK(ctx, cudaMemcpyAsync(ctx->h_best, ctx->d_best, sizeof(BestSlot), cudaMemcpyDeviceToHost, ctx->stream),
      "read result");
+  ctx->stats.d2h_bytes += sizeof(BestSlot);
   CK(ctx, cudaStreamSynchronize(ctx->stream), "scan");
+  float kms = 0.0f;
+  CK(ctx, cudaEventElapsedTime(&kms, ctx->ev_start, ctx->ev_stop), "event time");
+  ctx->stats.last_scan_kernel_ms = kms;
+  int64_t trip = 0;
+  for (int64_t i = ib; i < ie; i++) {
+    const int64_t r = m - 1 - i;
+    trip += r * (r - 1) / 2;
+  }
+  ctx->stats.last_scan_triplets = trip;
+  ctx->stats.last_scan_words = d.w0 + d.w1;
   *best_out = *ctx->h_best;
   if (top_k > 1) {
     std::vector<BestSlot> cand((size_t)n_warps * 32);
-    CK(ctx, cudaMemcpy(cand.data(), ctx->d_cand, cand.size() * sizeof(BestSlot), cudaMemcpyDeviceToHost),
+    CK(ctx, cudaMemcpyAsync(cand.data(), ctx->d_cand, cand.size() * sizeof(BestSlot), cudaMemcpyDeviceToHost,
+                            ctx->stream),
        "read candidates");
+    CK(ctx, cudaStreamSynchronize(ctx->stream), "read candidates");
+    ctx->stats.d2h_bytes += cand.size() * sizeof(BestSlot);
     std::sort(cand.begin(), cand.end(), [](const BestSlot& a, const BestSlot& b) {
       return a.score < b.score || (a.score == b.score && a.key < b.key);
     });
@@ -237,7 +260,12 @@ int epik2_create(epik2_ctx** out, int device) {
   if (cudaSetDevice(device) != cudaSuccess) return EPIK2_E_NO_DEVICE;
   if (cudaGetDeviceProperties(&ctx->prop, device) != cudaSuccess) return EPIK2_E_NO_DEVICE;
   if (ctx->prop.major != 10) return EPIK2_E_NO_DEVICE;  // built for sm_100a only
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return EPIK2_E_CUDA;
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) return EPIK2_E_CUDA;
+  ctx->stream = ctx->own_stream;
+  if (cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev_stop) != cudaSuccess) {
+    epik2_destroy(ctx.release());
+    return EPIK2_E_CUDA;
+  }
   ctx->scan_blocks = ctx->prop.multiProcessorCount * scan_blocks_per_sm();
   const int n_warps = ctx->scan_blocks * (kScanThreads / 32);
   if (cudaMalloc(&ctx->d_counter, 64) != cudaSuccess || cudaMalloc(&ctx->d_slots, sizeof(BestSlot) * n_warps) ||
@@ -262,7 +290,9 @@ void epik2_destroy(epik2_ctx* ctx) {
   cudaFree(ctx->d_cand);
   cudaFree(ctx->d_pgoff);
   cudaFreeHost(ctx->h_best);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+  if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
 
@@ -276,6 +306,32 @@ int epik2_mem_info(const epik2_ctx* ctx, size_t* free_bytes, size_t* total_bytes
   if (!ctx || !free_bytes || !total_bytes) return EPIK2_E_INVALID;
   cudaSetDevice(ctx->device);
   return cudaMemGetInfo(free_bytes, total_bytes) == cudaSuccess ? EPIK2_OK : EPIK2_E_CUDA;
+}
+
+int epik2_set_stream(epik2_ctx* ctx, void* cuda_stream) {
+  if (!ctx) return EPIK2_E_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->stream = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own_stream;
+  return EPIK2_OK;
+}
+
+int epik2_get_stream(const epik2_ctx* ctx, void** cuda_stream) {
+  if (!ctx || !cuda_stream) return EPIK2_E_INVALID;
+  *cuda_stream = (void*)ctx->stream;
+  return EPIK2_OK;
+}
+
+int epik2_get_stats(const epik2_ctx* ctx, epik2_stats* out) {
+  if (!ctx || !out) return EPIK2_E_INVALID;
+  *out = ctx->stats;
+  return EPIK2_OK;
+}
+
+int epik2_reset_stats(epik2_ctx* ctx) {
+  if (!ctx) return EPIK2_E_INVALID;
+  ctx->stats = epik2_stats{};
+  return EPIK2_OK;
 }
 
 int epik2_generate_reference(int64_t n_samples, int64_t n_snps, uint8_t* geno, uint8_t* pheno) {
@@ -335,6 +391,7 @@ int epik2_load_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int
   cudaError_t e = cudaMemcpyAsync(d->geno, geno, (size_t)(n_samples * n_snps), cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d->lut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+  ctx->stats.h2d_bytes += (uint64_t)(n_samples * n_snps) + lut.size() * 4;
   if (e != cudaSuccess) {
     cudaFree(d->block);
     return cuda_fail(ctx, e, "upload dataset");
@@ -449,6 +506,7 @@ int epik2_dump_tables(epik2_ctx* ctx, int32_t dataset_id, uint32_t* tables, floa
     e = cudaSuccess;
     if (tables) e = cudaMemcpy(tables, dt, (size_t)T * 54 * 4, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && scores) e = cudaMemcpy(scores, ds, (size_t)T * 4, cudaMemcpyDeviceToHost);
+    ctx->stats.d2h_bytes += (tables ? (uint64_t)T * 54 * 4 : 0) + (scores ? (uint64_t)T * 4 : 0);
     if (e != cudaSuccess) r = cuda_fail(ctx, e, "read dump");
   }
   cudaFree(dt);
@@ -472,6 +530,9 @@ int epik2_tables(epik2_ctx* ctx, int32_t dataset_id, const uint32_t* triplets, i
   cudaError_t e = cudaMalloc(&dout, (size_t)n * 54 * 4);
   if (e == cudaSuccess) e = cudaMemcpy(dtrip, triplets, (size_t)n * 12, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = launch_tables(*d, dtrip, n, dout, ctx->stream);
+  ctx->stats.kernel_launches += 1;
+  ctx->stats.h2d_bytes += (uint64_t)n * 12;
+  ctx->stats.d2h_bytes += (uint64_t)n * 54 * 4;
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpy(tables, dout, (size_t)n * 54 * 4, cudaMemcpyDeviceToHost);
   cudaFree(dtrip);

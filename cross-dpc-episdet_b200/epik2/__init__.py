@@ -48,6 +48,15 @@ class Best(ctypes.Structure):
         return f"Best(score={self.score!r}, score_fp64={self.score_fp64!r}, ijk={self.ijk})"
 
 
+class Stats(ctypes.Structure):
+    _fields_ = [("kernel_launches", ctypes.c_uint64), ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+                ("last_scan_kernel_ms", ctypes.c_double), ("last_scan_triplets", ctypes.c_int64),
+                ("last_scan_words", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class Opts(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("top_k", ctypes.c_int32), ("rescore_fp64", ctypes.c_int32),
                 ("k_strip", ctypes.c_int32), ("pairs_per_warp", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
@@ -57,9 +66,13 @@ class Opts(ctypes.Structure):
 _lib = None
 
 
-def exported_symbols():
-    """Function names declared in include/epik2.h."""
-    with open(HEADER) as f:
+PROBE_LIB_PATH = os.path.join(HERE, "lib", "libepik2_probe.so")
+PROBE_HEADER = os.path.join(REPO_ROOT, "include", "epik2_probe.h")
+
+
+def exported_symbols(header=HEADER):
+    """Function names declared in a header of include/."""
+    with open(header) as f:
         text = f.read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(epik2_[a-z0-9_]+)\s*\(", text)))
@@ -96,6 +109,10 @@ def library():
         "epik2_dump_tables": ([p, i32, p, p], ctypes.c_int),
         "epik2_tables": ([p, i32, p, i64, p], ctypes.c_int),
         "epik2_k2_lut": ([i64, p], ctypes.c_int),
+        "epik2_set_stream": ([p, p], ctypes.c_int),
+        "epik2_get_stream": ([p, ctypes.POINTER(p)], ctypes.c_int),
+        "epik2_get_stats": ([p, ctypes.POINTER(Stats)], ctypes.c_int),
+        "epik2_reset_stats": ([p], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -191,6 +208,23 @@ class Context:
     def handle(self):
         return self._h
 
+    def stats(self):
+        st = Stats()
+        self._check(self._lib.epik2_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        self._check(self._lib.epik2_reset_stats(self._h))
+
+    def stream(self):
+        """The cudaStream_t (as an int) the context launches on."""
+        v = ctypes.c_void_p()
+        self._check(self._lib.epik2_get_stream(self._h, ctypes.byref(v)))
+        return v.value or 0
+
+    def set_stream(self, stream_ptr):
+        self._check(self._lib.epik2_set_stream(self._h, ctypes.c_void_p(stream_ptr or None)))
+
     def device_name(self):
         buf = ctypes.create_string_buffer(256)
         self._check(self._lib.epik2_device_name(self._h, buf, 256))
@@ -266,3 +300,18 @@ class Context:
         out = np.zeros((len(t), 54), dtype=np.uint32)
         self._check(self._lib.epik2_tables(self._h, dataset, _ptr(t), len(t), _ptr(out)))
         return out
+
+
+def probe_int_peaks(device=0):
+    """Measured POPC / LOP3 / IADD rates of the device, operations per second."""
+    if not os.path.exists(PROBE_LIB_PATH):
+        raise Epik2Error(E_NO_DEVICE, f"{PROBE_LIB_PATH} not built")
+    L = ctypes.CDLL(PROBE_LIB_PATH)
+    d = ctypes.POINTER(ctypes.c_double)
+    L.epik2_probe_int_peaks.argtypes = [ctypes.c_int, d, d, d]
+    L.epik2_probe_int_peaks.restype = ctypes.c_int
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    r = L.epik2_probe_int_peaks(device, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    if r:
+        raise Epik2Error(r, "probe failed")
+    return {"popc_per_s": a.value, "lop3_per_s": b.value, "iadd_per_s": c.value}

@@ -91,6 +91,25 @@ int epik2_device_name(const epik2_ctx *ctx, char *buf, size_t len);
 /* Bytes of device memory currently free / total on the context's device. */
 int epik2_mem_info(const epik2_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
 
+/* Run the context's work on a caller-owned stream (e.g. a PyTorch stream); NULL restores
+ * the context's own stream.  The library still synchronises that stream before it
+ * returns results to the host. */
+int epik2_set_stream(epik2_ctx *ctx, void *cuda_stream);
+int epik2_get_stream(const epik2_ctx *ctx, void **cuda_stream);
+
+/* Counters kept by the context (no reference counterpart: the reference's only
+ * instrument is a TSC timer around its launch loop, GPU/v4.cpp:282, 609). */
+typedef struct {
+  uint64_t kernel_launches;     /* CUDA kernels this library launched on the context */
+  uint64_t h2d_bytes;           /* bytes copied host -> device */
+  uint64_t d2h_bytes;           /* bytes copied device -> host */
+  double last_scan_kernel_ms;   /* device time of the last search kernel (CUDA events on its stream) */
+  int64_t last_scan_triplets;   /* triplets scored by the last search */
+  int64_t last_scan_words;      /* 32-sample class words per triplet in the last search (both classes) */
+} epik2_stats;
+int epik2_get_stats(const epik2_ctx *ctx, epik2_stats *out);
+int epik2_reset_stats(epik2_ctx *ctx);
+
 /* --------------------------------------------------------------------------------
  * Data sources (host).  The reference synthesises its input inside main().
  * ------------------------------------------------------------------------------ */

@@ -1,0 +1,21 @@
+/*
+ * epik2_probe.h -- measured integer-pipe peaks of a device (libepik2_probe.so).
+ *
+ * No reference counterpart.  The roofline of the integer search kernel is the POPC
+ * issue rate, which no vendor table gives for this GPU; these probes measure it (and
+ * the LOP3 and IADD rates) with independent instruction chains on every SM, timed with
+ * CUDA events.  Each probe runs about 10-30 ms.
+ */
+#ifndef EPIK2_PROBE_H
+#define EPIK2_PROBE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Results in instructions per second per device (thread-level operations). */
+int epik2_probe_int_peaks(int device, double *popc_per_s, double *lop3_per_s, double *iadd_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -25,6 +25,14 @@ def test_library_exports_every_declared_symbol():
     assert set(declared) <= exported
 
 
+def test_probe_library_exports_every_declared_symbol():
+    import ctypes as C
+    lib = C.CDLL(epik2.PROBE_LIB_PATH)
+    declared = epik2.exported_symbols(epik2.PROBE_HEADER)
+    assert declared == ["epik2_probe_int_peaks"]
+    assert all(hasattr(lib, s) for s in declared)
+
+
 def test_strerror_and_invalid_arguments():
     lib = epik2.library()
     assert epik2.strerror(0) == "ok"
