@@ -268,6 +268,13 @@ def run_ours(args, rank, world, local_rank):
     # roofline of the search kernel: algorithmic popcounts (8 per triplet per 32-sample
     # class word) over the kernel's own event-timed duration, against the measured POPC rate
     achieved_popc = popc_local / (sum(kernel_ms) / 1e3)
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["k_scan_int"]
+        if tr["workload"] == cfg["name"]:
+            traffic = tr["dram_bytes_per_triplet"] * sum(step_trip) / len(step_trip)
+    except (OSError, KeyError, ValueError):
+        pass
     ref_form_popc = sum(step_trip) * words * 27 / (sum(kernel_ms) / 1e3)
 
     # end to end through the one-call entry point, pinned host buffers
@@ -327,7 +334,8 @@ def run_ours(args, rank, world, local_rank):
                        "l2": f"flushed before every step ({args.flush_mb} MiB write)",
                        "parallelism": f"{world} GPU(s), shard-parallel", "engine": "integer (LOP3+POPC)"},
             "roofline": {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": peaks["popc_per_s"] / 1e9,
-                         "unit": "Gpopc/s", "frac": achieved_popc / peaks["popc_per_s"], "traffic": None,
+                         "unit": "Gpopc/s", "frac": achieved_popc / peaks["popc_per_s"], "traffic": traffic,
+                         "traffic_source": "ncu dram bytes per triplet (profiles/traffic.json) x triplets per launch",
                          "peak_source": "measured live by epik2_probe_int_peaks on this GPU",
                          "algorithmic_popc_per_triplet_word": 8,
                          "reference_form_frac": ref_form_popc / peaks["popc_per_s"],
