@@ -76,6 +76,7 @@ int scan_blocks_per_sm();
 
 // Host helpers (host_data.cpp).
 void build_k2_lut(int64_t n_max, float* lut);
+void build_k2_lut_range(int64_t n_begin, int64_t n_end, float* out);  // out[n - n_begin], n in [begin, end)
 void generate_reference(int64_t n, int64_t m, uint8_t* geno, uint8_t* pheno);
 void generate_hwe(uint64_t seed, int64_t n, int64_t m, int64_t n_cases, double maf_lo, double maf_hi,
                   int n_planted, const int64_t* planted, const double* effects, uint8_t* geno, uint8_t* pheno);

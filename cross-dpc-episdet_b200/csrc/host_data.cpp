@@ -19,23 +19,25 @@ namespace epik2 {
 // The reference's GPU kernels evaluate the Stirling tail in float with the SYCL device
 // log/exp (GPU/v4.cpp:52-61); that arithmetic is not reproducible here, so the search
 // follows the CPU path, which the reference's CPU programs all share.
-void build_k2_lut(int64_t n_max, float* lut) {
+void build_k2_lut_range(int64_t n_begin, int64_t n_end, float* out) {
   const double table_error = -0.0810;  // TABLE_ERROR, GPU/v4.cpp:16
   float t[kTableMaxSize];
   t[0] = 0.0f;
   t[1] = 0.0f;
   for (int n = 2; n < kTableMaxSize; n++) t[n] = (float)((double)t[n - 1] + std::log((double)n));
   const double log_e = std::log(std::exp(1.0));
-  for (int64_t n = 0; n <= n_max; n++) {
+  for (int64_t n = n_begin; n < n_end; n++) {
     if (n < kTableMaxSize) {
-      lut[n] = t[n];
+      out[n - n_begin] = t[n];
     } else {
       double a = ((double)n + 0.5) * std::log((double)n);
       double b = (double)(n - 1) * log_e;
-      lut[n] = (float)(a - b + table_error);
+      out[n - n_begin] = (float)(a - b + table_error);
     }
   }
 }
+
+void build_k2_lut(int64_t n_max, float* lut) { build_k2_lut_range(0, n_max + 1, lut); }
 
 // The reference's synthetic input (GPU/v4.cpp:81-110): srand(100); rand()%3 per
 // genotype in sample-major order; exactly n/2 cases by rejection sampling.  An index

@@ -113,6 +113,7 @@ def library():
         "epik2_get_stream": ([p, ctypes.POINTER(p)], ctypes.c_int),
         "epik2_get_stats": ([p, ctypes.POINTER(Stats)], ctypes.c_int),
         "epik2_reset_stats": ([p], ctypes.c_int),
+        "epik2_scan_u8_noalloc": ([p, p, i64, i64, p, ctypes.POINTER(Best)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -153,6 +154,24 @@ def generate_hwe(seed, n_samples, n_snps, n_cases, maf=(0.05, 0.5), planted=(), 
     if r:
         raise Epik2Error(r, strerror(r))
     return g, ph
+
+
+NOALLOC_SCRATCH_BYTES = 64 << 20
+
+
+def scan_u8_noalloc(geno, pheno, stream=None):
+    """Allocation-free one-call search on the current device (epik2_scan_u8_noalloc).
+
+    For callers that cannot allocate device memory: all intermediates live in the
+    library's fixed 64 MiB static device array.  Raises Epik2Error on failure."""
+    geno = np.ascontiguousarray(geno, dtype=np.uint8)
+    pheno = np.ascontiguousarray(pheno, dtype=np.uint8)
+    b = Best()
+    r = library().epik2_scan_u8_noalloc(_ptr(geno), _ptr(pheno), geno.shape[0], geno.shape[1],
+                                        ctypes.c_void_p(stream or None), ctypes.byref(b))
+    if r:
+        raise Epik2Error(r, strerror(r))
+    return b
 
 
 def k2_lut(n_max):

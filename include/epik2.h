@@ -166,6 +166,26 @@ int epik2_tables(epik2_ctx *ctx, int32_t dataset_id, const uint32_t *triplets, i
 /* The FP32 log-factorial lookup table used by the score, lut[0..n_max]. */
 int epik2_k2_lut(int64_t n_max, float *lut);
 
+/* --------------------------------------------------------------------------------
+ * Allocation-free search.  No counterpart in the reference.
+ * ------------------------------------------------------------------------------ */
+#define EPIK2_NOALLOC_SCRATCH_BYTES (64u << 20)
+/* Same result as epik2_scan_u8, for callers that cannot allocate device memory -- e.g.
+ * code running inside a host application that owns the device heap, or under a device
+ * memory budget fixed before this library is reached.  Creates no context and calls no
+ * cudaMalloc/cudaFree or other allocating routine: every intermediate lives in one static
+ * device array of EPIK2_NOALLOC_SCRATCH_BYTES (64 MiB) that each GPU loading this library
+ * holds until the process exits.  Runs on the current device, on `cuda_stream` (NULL =
+ * the default stream), and returns once the result is on the host.
+ *   - The first call on a device looks up the array's device address; make that first
+ *     call before any stream capture.
+ *   - All calls share the array, which keeps the last call's contents (each call clears
+ *     what must start at zero).  Calls whose GPU work overlaps race on it.
+ *   - Shapes whose buffers do not fit (about n_samples*n_snps + 16*n_snps^2 bytes plus
+ *     n_samples*n_snps/4) or with more than 4096 SNPs return EPIK2_E_TOO_LARGE. */
+int epik2_scan_u8_noalloc(const uint8_t *geno, const uint8_t *pheno, int64_t n_samples, int64_t n_snps,
+                          void *cuda_stream, epik2_best *out);
+
 #ifdef __cplusplus
 }
 #endif
