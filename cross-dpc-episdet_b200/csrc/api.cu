@@ -31,6 +31,7 @@ struct epik2_ctx {
   BestSlot* d_slots = nullptr;  // one per warp of the scan grid
   BestSlot* d_best = nullptr;
   BestSlot* d_cand = nullptr;   // 32 per warp (top-k form)
+  Rescored* d_resc = nullptr;   // FP64 rescore of every candidate
   int64_t* d_pgoff = nullptr;
   int64_t pgoff_cap = 0;
   BestSlot* h_best = nullptr;   // pinned
@@ -60,7 +61,7 @@ int cuda_fail(epik2_ctx* ctx, cudaError_t e, const char* what) {
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
-  size_t geno, perm, planes, singles, pairs, lut, total;
+  size_t geno, perm, planes, singles, pairs, lut, lut64, total;
 };
 
 Layout dataset_layout(int64_t s, int64_t m) {
@@ -80,6 +81,8 @@ Layout dataset_layout(int64_t s, int64_t m) {
   off = align_up(off + (size_t)(2 * tri_size(m_pad)) * 16, 256);
   L.lut = off;
   off = align_up(off + (size_t)(s + 2) * 4, 256);
+  L.lut64 = off;
+  off = align_up(off + (size_t)(s + 2) * 8, 256);
   L.total = off;
   return L;
 }
@@ -204,7 +207,32 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   ctx->stats.last_scan_triplets = trip;
   ctx->stats.last_scan_words = d.w0 + d.w1;
   *best_out = *ctx->h_best;
-  if (top_k > 1) {
+  const bool rescore = opts && opts->rescore_fp64;
+  if (top_k > 1 && rescore) {
+    const int64_t nc = (int64_t)n_warps * 32;
+    CK(ctx, launch_rescore(d, ctx->d_cand, nc, ctx->d_resc, ctx->stream), "rescore kernel");
+    ctx->stats.kernel_launches += 1;
+    std::vector<Rescored> res((size_t)nc);
+    CK(ctx, cudaMemcpyAsync(res.data(), ctx->d_resc, res.size() * sizeof(Rescored), cudaMemcpyDeviceToHost,
+                            ctx->stream),
+       "read rescored");
+    CK(ctx, cudaStreamSynchronize(ctx->stream), "rescore");
+    ctx->stats.d2h_bytes += res.size() * sizeof(Rescored);
+    std::sort(res.begin(), res.end(), [](const Rescored& a, const Rescored& b) {
+      const bool va = a.key != ~0ull, vb = b.key != ~0ull;
+      if (va != vb) return va;
+      return a.s64 < b.s64 || (a.s64 == b.s64 && a.key < b.key);
+    });
+    ctx->last_topk.clear();
+    for (const Rescored& c : res) {
+      if ((int)ctx->last_topk.size() >= top_k || c.key == ~0ull) break;
+      epik2_best e{};
+      e.score = c.s32;
+      e.score_fp64 = c.s64;
+      decode_key(c.key, e.i, e.j, e.k);
+      ctx->last_topk.push_back(e);
+    }
+  } else if (top_k > 1) {
     std::vector<BestSlot> cand((size_t)n_warps * 32);
     CK(ctx, cudaMemcpyAsync(cand.data(), ctx->d_cand, cand.size() * sizeof(BestSlot), cudaMemcpyDeviceToHost,
                             ctx->stream),
@@ -270,6 +298,7 @@ int epik2_create(epik2_ctx** out, int device) {
   const int n_warps = ctx->scan_blocks * (kScanThreads / 32);
   if (cudaMalloc(&ctx->d_counter, 64) != cudaSuccess || cudaMalloc(&ctx->d_slots, sizeof(BestSlot) * n_warps) ||
       cudaMalloc(&ctx->d_best, sizeof(BestSlot)) || cudaMalloc(&ctx->d_cand, sizeof(BestSlot) * n_warps * 32) ||
+      cudaMalloc(&ctx->d_resc, sizeof(Rescored) * n_warps * 32) ||
       cudaMallocHost(&ctx->h_best, sizeof(BestSlot))) {
     epik2_destroy(ctx.release());
     return EPIK2_E_NOMEM;
@@ -288,6 +317,7 @@ void epik2_destroy(epik2_ctx* ctx) {
   cudaFree(ctx->d_slots);
   cudaFree(ctx->d_best);
   cudaFree(ctx->d_cand);
+  cudaFree(ctx->d_resc);
   cudaFree(ctx->d_pgoff);
   cudaFreeHost(ctx->h_best);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
@@ -386,12 +416,17 @@ int epik2_load_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int
   d->singles = (uint32_t*)(b + L.singles);
   d->pairs = (uint4*)(b + L.pairs);
   d->lut = (float*)(b + L.lut);
+  d->lut64 = (double*)(b + L.lut64);
   std::vector<float> lut((size_t)n_samples + 2);
   build_k2_lut(n_samples + 1, lut.data());
+  std::vector<double> lut64((size_t)n_samples + 2);
+  build_k2_lut64(n_samples + 1, lut64.data());
   cudaError_t e = cudaMemcpyAsync(d->geno, geno, (size_t)(n_samples * n_snps), cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d->lut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
-  ctx->stats.h2d_bytes += (uint64_t)(n_samples * n_snps) + lut.size() * 4;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d->lut64, lut64.data(), lut64.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+  ctx->stats.h2d_bytes += (uint64_t)(n_samples * n_snps) + lut.size() * 4 + lut64.size() * 8;
   if (e != cudaSuccess) {
     cudaFree(d->block);
     return cuda_fail(ctx, e, "upload dataset");
@@ -448,12 +483,20 @@ int epik2_scan(epik2_ctx* ctx, int32_t dataset_id, const epik2_opts* opts, epik2
   if (d->n_snps < 3) return fail(ctx, EPIK2_E_INVALID, "need at least 3 SNPs");
   CK(ctx, cudaSetDevice(ctx->device), "set device");
   BestSlot b{};
-  int r = run_scan(ctx, *d, opts, nullptr, nullptr, &b);
+  epik2_opts o{};
+  if (opts) o = *opts;
+  if (o.rescore_fp64 && o.top_k < 2) o.top_k = 32;
+  int r = run_scan(ctx, *d, &o, nullptr, nullptr, &b);
   if (r) return r;
+  if (b.key == ~0ull) return fail(ctx, EPIK2_E_INVALID, "no triplet in the requested range");
+  if (o.rescore_fp64) {
+    if (ctx->last_topk.empty()) return fail(ctx, EPIK2_E_CUDA, "rescore produced no candidate");
+    *out = ctx->last_topk[0];  // best by FP64 score
+    return EPIK2_OK;
+  }
   out->score = b.score;
   out->score_fp64 = std::numeric_limits<double>::quiet_NaN();
   decode_key(b.key, out->i, out->j, out->k);
-  if (b.key == ~0ull) return fail(ctx, EPIK2_E_INVALID, "no triplet in the requested range");
   return EPIK2_OK;
 }
 

@@ -24,6 +24,7 @@ struct DevDataset {
   uint32_t* singles = nullptr;  // [2][m_pad][2] counts of g0, g1 per class
   uint4* pairs = nullptr;       // [2][tri(m_pad)] counts (00,01,10,11) for x<y
   float* lut = nullptr;         // ln n! in the reference CPU arithmetic, [0, n_samples+1]
+  double* lut64 = nullptr;      // ln n! in double (precision form), [0, n_samples+1]
   int64_t tri = 0;              // entries per class in `pairs`
   void* block = nullptr;        // single allocation holding all of the above
   size_t bytes = 0;
@@ -45,6 +46,14 @@ struct BestSlot {
 __host__ __device__ inline unsigned long long pack_key(uint64_t i, uint64_t j, uint64_t k) {
   return (i << 42) | (j << 21) | k;
 }
+
+// FP64 rescore of one candidate.
+struct Rescored {
+  double s64;
+  float s32;
+  uint32_t pad;
+  unsigned long long key;
+};
 
 struct ScanParams {
   const uint2* planes;
@@ -72,11 +81,13 @@ cudaError_t launch_scan_int(const ScanParams& p, int blocks, bool dump, cudaStre
 cudaError_t launch_reduce_best(const BestSlot* slots, int n, BestSlot* out, cudaStream_t stream);
 cudaError_t launch_tables(const DevDataset& d, const uint32_t* triplets, int64_t n, uint32_t* out,
                           cudaStream_t stream);
+cudaError_t launch_rescore(const DevDataset& d, const BestSlot* cand, int64_t n, Rescored* out, cudaStream_t stream);
 int scan_blocks_per_sm();
 
 // Host helpers (host_data.cpp).
 void build_k2_lut(int64_t n_max, float* lut);
 void build_k2_lut_range(int64_t n_begin, int64_t n_end, float* out);  // out[n - n_begin], n in [begin, end)
+void build_k2_lut64(int64_t n_max, double* lut);
 void generate_reference(int64_t n, int64_t m, uint8_t* geno, uint8_t* pheno);
 void generate_hwe(uint64_t seed, int64_t n, int64_t m, int64_t n_cases, double maf_lo, double maf_hi,
                   int n_planted, const int64_t* planted, const double* effects, uint8_t* geno, uint8_t* pheno);

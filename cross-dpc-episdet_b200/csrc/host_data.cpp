@@ -39,6 +39,22 @@ void build_k2_lut_range(int64_t n_begin, int64_t n_end, float* out) {
 
 void build_k2_lut(int64_t n_max, float* lut) { build_k2_lut_range(0, n_max + 1, lut); }
 
+// The same ln n! evaluated entirely in double (precision form's FP64 rescore): the table
+// part accumulated in double, the Stirling tail in double and not rounded to float.
+void build_k2_lut64(int64_t n_max, double* lut) {
+  const double table_error = -0.0810;
+  const double log_e = std::log(std::exp(1.0));
+  double acc = 0.0;
+  for (int64_t n = 0; n <= n_max; n++) {
+    if (n < kTableMaxSize) {
+      if (n >= 2) acc += std::log((double)n);
+      lut[n] = acc;
+    } else {
+      lut[n] = ((double)n + 0.5) * std::log((double)n) - (double)(n - 1) * log_e + table_error;
+    }
+  }
+}
+
 // The reference's synthetic input (GPU/v4.cpp:81-110): srand(100); rand()%3 per
 // genotype in sample-major order; exactly n/2 cases by rejection sampling.  An index
 // equal to n (rand()==RAND_MAX) is dropped, which is where the reference's write lands

@@ -305,22 +305,19 @@ __global__ void k_reduce_best(const BestSlot* __restrict__ slots, int n, BestSlo
   }
 }
 
-// Tables of an explicit triplet list, one warp per triplet, all 27 cells per class
-// popcounted directly as in the reference (GPU/v2.cpp:288-540) -- an independent check
-// of the inclusion-exclusion path.  g2 = ~(g0|g1) restricted to the valid bits of the
-// class's last word.
-__global__ void k_tables_direct(const uint2* __restrict__ planes, int64_t m_pad, int64_t w0, int64_t w1, int64_t n0,
-                                int64_t n1, const uint32_t* __restrict__ trip, int64_t n, uint32_t* __restrict__ out) {
-  const int lane = threadIdx.x & 31;
-  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (t >= n) return;
-  const int64_t i = trip[3 * t], j = trip[3 * t + 1], k = trip[3 * t + 2];
+// 54-cell table of (i,j,k) by one warp, all 27 cells per class popcounted directly as in
+// the reference (GPU/v2.cpp:288-540) -- an independent check of the inclusion-exclusion
+// path.  g2 = ~(g0|g1) restricted to the valid bits of the class's last word.  Every lane
+// returns the full counts.
+__device__ __forceinline__ void warp_direct_table(const uint2* __restrict__ planes, int64_t m_pad, int64_t w0,
+                                                  int64_t w1, int64_t n0, int64_t n1, int64_t i, int64_t j, int64_t k,
+                                                  int lane, uint32_t (&cnt)[54]) {
+#pragma unroll
+  for (int c = 0; c < 54; c++) cnt[c] = 0;
+#pragma unroll
   for (int cl = 0; cl < 2; cl++) {
     const int64_t wb = cl ? w0 : 0, we = cl ? w0 + w1 : w0;
     const int64_t ncls = cl ? n1 : n0;
-    uint32_t cnt[27];
-#pragma unroll
-    for (int c = 0; c < 27; c++) cnt[c] = 0;
     for (int64_t w = wb + lane; w < we; w += 32) {
       const int64_t bits_left = ncls - 32 * (w - wb);
       const uint32_t valid = bits_left >= 32 ? 0xffffffffu : ((1u << bits_left) - 1u);
@@ -333,15 +330,63 @@ __global__ void k_tables_direct(const uint2* __restrict__ planes, int64_t m_pad,
 #pragma unroll
         for (int y = 0; y < 3; y++)
 #pragma unroll
-          for (int z = 0; z < 3; z++) cnt[9 * x + 3 * y + z] += __popc(ga[x] & gb[y] & gc[z]);
+          for (int z = 0; z < 3; z++) cnt[27 * cl + 9 * x + 3 * y + z] += __popc(ga[x] & gb[y] & gc[z]);
     }
+  }
+#pragma unroll
+  for (int c = 0; c < 54; c++) {
+    uint32_t v = cnt[c];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+    cnt[c] = v;
+  }
+}
+
+__global__ void k_tables_direct(const uint2* __restrict__ planes, int64_t m_pad, int64_t w0, int64_t w1, int64_t n0,
+                                int64_t n1, const uint32_t* __restrict__ trip, int64_t n, uint32_t* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (t >= n) return;
+  uint32_t cnt[54];
+  warp_direct_table(planes, m_pad, w0, w1, n0, n1, trip[3 * t], trip[3 * t + 1], trip[3 * t + 2], lane, cnt);
+  if (lane == 0)
+#pragma unroll
+    for (int c = 0; c < 54; c++) out[t * 54 + c] = cnt[c];
+}
+
+// Precision form: rescore candidates in FP64.  One warp per candidate recounts its
+// table directly, then lane 0 evaluates K2 twice: FP32 in the reference order (must
+// equal the search's score) and FP64 from a double ln n! table -- the only FP64 step.
+__global__ void k_rescore(const uint2* __restrict__ planes, int64_t m_pad, int64_t w0, int64_t w1, int64_t n0,
+                          int64_t n1, const BestSlot* __restrict__ cand, int64_t n, const float* __restrict__ lut32,
+                          const double* __restrict__ lut64, Rescored* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (t >= n) return;
+  const unsigned long long key = cand[t].key;
+  if (key == ~0ull) {
+    if (lane == 0) {
+      out[t].s64 = 0.0;
+      out[t].s32 = FLT_MAX;
+      out[t].key = key;
+    }
+    return;
+  }
+  const int64_t i = (int64_t)(key >> 42), j = (int64_t)((key >> 21) & 0x1fffff), k = (int64_t)(key & 0x1fffff);
+  uint32_t cnt[54];
+  warp_direct_table(planes, m_pad, w0, w1, n0, n1, i, j, k, lane, cnt);
+  if (lane == 0) {
+    float s32 = 0.0f;
+    double s64 = 0.0;
 #pragma unroll
     for (int c = 0; c < 27; c++) {
-      uint32_t v = cnt[c];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
-      if (lane == 0) out[t * 54 + 27 * cl + c] = v;
+      const uint32_t a = cnt[c], b = cnt[27 + c];
+      s32 = __fadd_rn(s32, __fsub_rn(__fsub_rn(lut32[a + b + 1], lut32[a]), lut32[b]));
+      s64 = __dadd_rn(s64, __dsub_rn(__dsub_rn(lut64[a + b + 1], lut64[a]), lut64[b]));
     }
+    out[t].s64 = fabs(s64);
+    out[t].s32 = fabsf(s32);
+    out[t].key = key;
   }
 }
 
@@ -361,6 +406,15 @@ cudaError_t launch_scan_int(const ScanParams& p, int blocks, bool dump, cudaStre
 
 cudaError_t launch_reduce_best(const BestSlot* slots, int n, BestSlot* out, cudaStream_t stream) {
   k_reduce_best<<<1, 1024, 0, stream>>>(slots, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rescore(const DevDataset& d, const BestSlot* cand, int64_t n, Rescored* out,
+                           cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  const int64_t threads = n * 32;
+  k_rescore<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(d.planes, d.m_pad, d.w0, d.w1, d.n_controls,
+                                                                  d.n_cases, cand, n, d.lut, d.lut64, out);
   return cudaGetLastError();
 }
 

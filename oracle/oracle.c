@@ -396,3 +396,32 @@ int64_t oracle_scan_u8(const uint8_t *A, const uint8_t *B, int64_t N, int64_t M,
   free(z);
   return T;
 }
+
+/* FP64 K2 of every triplet at its lexicographic index (precision-form oracle). */
+int64_t oracle_scan_fp64_u8(const uint8_t *A, const uint8_t *B, int64_t N, int64_t M, double *scores64,
+                            int n_threads) {
+  int64_t n1 = 0;
+  for (int64_t s = 0; s < N; s++) n1 += (B[s] == 1);
+  int64_t n0 = N - n1;
+  int64_t W0 = (n0 + 31) / 32, W1 = (n1 + 31) / 32;
+  uint32_t *z = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(M * W0 * 2 + 1));
+  uint32_t *o = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(M * W1 * 2 + 1));
+  oracle_encode(A, B, N, M, z, o, &n1);
+  (void)oracle_lnfact_fp64(0); /* initialise the table before the parallel region */
+  int64_t T = (M >= 3) ? M * (M - 1) * (M - 2) / 6 : 0;
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#pragma omp parallel for schedule(dynamic)
+#endif
+  for (int64_t i = 0; i < M - 2; i++) {
+    uint32_t ft[54];
+    for (int64_t j = i + 1; j < M - 1; j++)
+      for (int64_t k = j + 1; k < M; k++) {
+        oracle_table(z, o, n0, n1, i, j, k, ft);
+        scores64[oracle_triplet_index(M, i, j, k)] = oracle_k2_fp64(ft);
+      }
+  }
+  free(o);
+  free(z);
+  return T;
+}

@@ -50,6 +50,8 @@ def lib():
         L.oracle_scan.restype = i64
         L.oracle_scan_u8.argtypes = [p, p, i64, i64, p, p, p, p, ctypes.c_int]
         L.oracle_scan_u8.restype = i64
+        L.oracle_scan_fp64_u8.argtypes = [p, p, i64, i64, p, ctypes.c_int]
+        L.oracle_scan_fp64_u8.restype = i64
         _lib = L
     return _lib
 
@@ -143,6 +145,21 @@ def scan(A, B, with_tables=False, n_threads=0):
         out["tables"] = tables[:T]
         out["scores"] = scores[:T]
     return out
+
+
+def scan_fp64(A, B, n_threads=0):
+    """FP64 K2 of every triplet, in lexicographic order."""
+    A = np.ascontiguousarray(A, dtype=np.uint8)
+    B = np.ascontiguousarray(B, dtype=np.uint8)
+    S, M = A.shape
+    T = M * (M - 1) * (M - 2) // 6 if M >= 3 else 0
+    out = np.zeros(max(T, 1), dtype=np.float64)
+    lib().oracle_scan_fp64_u8(_ptr(A), _ptr(B), S, M, _ptr(out), n_threads)
+    return out[:T]
+
+
+def triplet_list(M):
+    return [(i, j, k) for i in range(M) for j in range(i + 1, M) for k in range(j + 1, M)]
 
 
 # ---------------------------------------------------------------- reference harnesses
