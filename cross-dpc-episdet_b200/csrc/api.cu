@@ -26,7 +26,14 @@ struct epik2_ctx {
   std::map<int32_t, std::unique_ptr<DevDataset>> datasets;
   int32_t next_id = 1;
   // search scratch
-  int scan_blocks = 0;
+  int engine = 0;               // default engine: 0 = auto (tensor cores), 1 = integer, 2 = tensor cores
+  int scan_blocks = 0;          // integer engine grid
+  int tc_blocks = 0;            // tensor-core engine grid (one CTA per SM)
+  int n_slots = 0;              // per-warp slots, enough for either grid
+  int* d_err = nullptr;
+  int64_t* d_pb_off = nullptr;
+  uint32_t* d_pb_ij = nullptr;
+  int64_t pb_cap = 0;
   unsigned long long* d_counter = nullptr;
   BestSlot* d_slots = nullptr;  // one per warp of the scan grid
   BestSlot* d_best = nullptr;
@@ -126,6 +133,19 @@ void decode_key(unsigned long long key, uint32_t& i, uint32_t& j, uint32_t& k) {
   k = (uint32_t)(key & ((1ull << 21) - 1));
 }
 
+int ensure_pb(epik2_ctx* ctx, int64_t n) {
+  if (n <= ctx->pb_cap) return EPIK2_OK;
+  cudaFree(ctx->d_pb_off);
+  cudaFree(ctx->d_pb_ij);
+  ctx->d_pb_off = nullptr;
+  ctx->d_pb_ij = nullptr;
+  ctx->pb_cap = 0;
+  CK(ctx, cudaMalloc(&ctx->d_pb_off, (size_t)(n + 1) * 8), "alloc tile list");
+  CK(ctx, cudaMalloc(&ctx->d_pb_ij, (size_t)n * 8), "alloc tile list");
+  ctx->pb_cap = n;
+  return EPIK2_OK;
+}
+
 int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
   if (n <= ctx->pgoff_cap) return EPIK2_OK;
   if (ctx->d_pgoff) cudaFree(ctx->d_pgoff);
@@ -135,6 +155,10 @@ int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
   ctx->pgoff_cap = n;
   return EPIK2_OK;
 }
+
+int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_k, int n_warps);
+int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts);
 
 // Pair groups of first index i: j0 = i+1, i+5, ... while j0 <= m-2.
 int64_t groups_of(int64_t m, int64_t i) { return (i <= m - 3) ? (m - 2 - i + kPairsPerWarp) / kPairsPerWarp : 0; }
@@ -151,9 +175,13 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
     }
     if (opts->top_k < 0 || opts->top_k > 32) return fail(ctx, EPIK2_E_INVALID, "top_k must be in [0, 32]");
     top_k = opts->top_k;
-    if (opts->engine != 0 && opts->engine != 1) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
+    if (opts->engine < 0 || opts->engine > 2) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
   }
   if (ie < ib) ie = ib;
+  int engine = ctx->engine;
+  if (opts && opts->engine != 0) engine = opts->engine;
+  if (engine == 0) engine = 2;
+  if (engine == 2) return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts);
   const int64_t n_first = std::max<int64_t>(ie - ib, 1);
   std::vector<int64_t> off((size_t)n_first + 1, 0);
   for (int64_t t = 0; t < n_first; t++) off[(size_t)t + 1] = off[(size_t)t] + (ib + t < ie ? groups_of(m, ib + t) : 0);
@@ -207,6 +235,10 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   ctx->stats.last_scan_triplets = trip;
   ctx->stats.last_scan_words = d.w0 + d.w1;
   *best_out = *ctx->h_best;
+  return collect_topk(ctx, d, opts, top_k, n_warps);
+}
+
+int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_k, int n_warps) {
   const bool rescore = opts && opts->rescore_fp64;
   if (top_k > 1 && rescore) {
     const int64_t nc = (int64_t)n_warps * 32;
@@ -255,6 +287,81 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   return EPIK2_OK;
 }
 
+// Tensor-core engine: one CTA per SM, tiles = pair blocks (i, j0..j0+31) x k blocks of 128.
+int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts) {
+  const int64_t m = d.n_snps;
+  const int64_t n_kb = (m + 127) / 128;
+  std::vector<uint32_t> ij;
+  std::vector<int64_t> off(1, 0);
+  for (int64_t i = ib; i < ie; i++)
+    for (int64_t j0 = i + 1; j0 <= m - 2; j0 += 32) {
+      ij.push_back((uint32_t)i);
+      ij.push_back((uint32_t)j0);
+      off.push_back(off.back() + (n_kb - (j0 + 1) / 128));
+    }
+  const int64_t n_pb = (int64_t)off.size() - 1;
+  int r = ensure_pb(ctx, std::max<int64_t>(n_pb, 1));
+  if (r) return r;
+  if (n_pb > 0) {
+    CK(ctx, cudaMemcpyAsync(ctx->d_pb_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, ctx->stream),
+       "upload tile list");
+    CK(ctx, cudaMemcpyAsync(ctx->d_pb_ij, ij.data(), ij.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
+       "upload tile list");
+    ctx->stats.h2d_bytes += off.size() * 8 + ij.size() * 4;
+  }
+  CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream), "reset counter");
+  CK(ctx, cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream), "reset error word");
+  TcParams p{};
+  p.planes = d.planes;
+  p.singles = d.singles;
+  p.pairs = d.pairs;
+  p.lut = d.lut;
+  p.pb_off = ctx->d_pb_off;
+  p.pb_ij = ctx->d_pb_ij;
+  p.n_pb = std::max<int64_t>(n_pb, 1);
+  p.n_tiles = off.back();
+  p.tri = d.tri;
+  p.m = (int32_t)m;
+  p.m_pad = (int32_t)d.m_pad;
+  p.w0 = (int32_t)d.w0;
+  p.w1 = (int32_t)d.w1;
+  p.n0 = (int32_t)d.n_controls;
+  p.n1 = (int32_t)d.n_cases;
+  p.counter = ctx->d_counter;
+  p.slots = ctx->d_slots;
+  p.top_k = top_k;
+  p.cand = ctx->d_cand;
+  p.dump_tables = dump_tables;
+  p.dump_scores = dump_scores;
+  p.err = ctx->d_err;
+  CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
+  CK(ctx, launch_scan_tc(p, ctx->tc_blocks, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
+  CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
+  const int n_warps = ctx->tc_blocks * tc_warps_per_block();
+  CK(ctx, launch_reduce_best(ctx->d_slots, n_warps, ctx->d_best, ctx->stream), "reduce kernel");
+  ctx->stats.kernel_launches += 2;
+  CK(ctx, cudaMemcpyAsync(ctx->h_best, ctx->d_best, sizeof(BestSlot), cudaMemcpyDeviceToHost, ctx->stream),
+     "read result");
+  int err_word = 0;
+  CK(ctx, cudaMemcpyAsync(&err_word, ctx->d_err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read error word");
+  ctx->stats.d2h_bytes += sizeof(BestSlot) + 4;
+  CK(ctx, cudaStreamSynchronize(ctx->stream), "scan");
+  if (err_word) return fail(ctx, EPIK2_E_TIMEOUT, "tensor-core scan: a bounded wait expired");
+  float kms = 0.0f;
+  CK(ctx, cudaEventElapsedTime(&kms, ctx->ev_start, ctx->ev_stop), "event time");
+  ctx->stats.last_scan_kernel_ms = kms;
+  int64_t trip = 0;
+  for (int64_t i = ib; i < ie; i++) {
+    const int64_t rr = m - 1 - i;
+    trip += rr * (rr - 1) / 2;
+  }
+  ctx->stats.last_scan_triplets = trip;
+  ctx->stats.last_scan_words = d.w0 + d.w1;
+  *best_out = *ctx->h_best;
+  return collect_topk(ctx, d, opts, top_k, n_warps);
+}
+
 }  // namespace
 
 extern "C" {
@@ -295,8 +402,10 @@ int epik2_create(epik2_ctx** out, int device) {
     return EPIK2_E_CUDA;
   }
   ctx->scan_blocks = ctx->prop.multiProcessorCount * scan_blocks_per_sm();
-  const int n_warps = ctx->scan_blocks * (kScanThreads / 32);
-  if (cudaMalloc(&ctx->d_counter, 64) != cudaSuccess || cudaMalloc(&ctx->d_slots, sizeof(BestSlot) * n_warps) ||
+  ctx->tc_blocks = ctx->prop.multiProcessorCount;
+  const int n_warps = std::max(ctx->scan_blocks * (kScanThreads / 32), ctx->tc_blocks * tc_warps_per_block());
+  ctx->n_slots = n_warps;
+  if (cudaMalloc(&ctx->d_counter, 64) != cudaSuccess || cudaMalloc(&ctx->d_err, 64) != cudaSuccess || cudaMalloc(&ctx->d_slots, sizeof(BestSlot) * n_warps) ||
       cudaMalloc(&ctx->d_best, sizeof(BestSlot)) || cudaMalloc(&ctx->d_cand, sizeof(BestSlot) * n_warps * 32) ||
       cudaMalloc(&ctx->d_resc, sizeof(Rescored) * n_warps * 32) ||
       cudaMallocHost(&ctx->h_best, sizeof(BestSlot))) {
@@ -319,6 +428,9 @@ void epik2_destroy(epik2_ctx* ctx) {
   cudaFree(ctx->d_cand);
   cudaFree(ctx->d_resc);
   cudaFree(ctx->d_pgoff);
+  cudaFree(ctx->d_err);
+  cudaFree(ctx->d_pb_off);
+  cudaFree(ctx->d_pb_ij);
   cudaFreeHost(ctx->h_best);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
@@ -343,6 +455,13 @@ int epik2_set_stream(epik2_ctx* ctx, void* cuda_stream) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   ctx->stream = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own_stream;
+  return EPIK2_OK;
+}
+
+int epik2_set_engine(epik2_ctx* ctx, int engine) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (engine < EPIK2_ENGINE_AUTO || engine > EPIK2_ENGINE_TC) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
+  ctx->engine = engine;
   return EPIK2_OK;
 }
 

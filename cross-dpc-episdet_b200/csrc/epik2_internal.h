@@ -74,7 +74,29 @@ struct ScanParams {
   float* dump_scores;      // [C(m,3)] or null
 };
 
-// Kernel launchers (scan_int.cu / encode.cu); all asynchronous on `stream`.
+// Tensor-core engine parameters (scan_tc.cu).  Tiles: for each pair block (i, j0..j0+31)
+// the k blocks [128*kb, 128*kb+128) with kb from (j0+1)/128 to ceil(m/128)-1.
+struct TcParams {
+  const uint2* planes;
+  const uint32_t* singles;
+  const uint4* pairs;
+  const float* lut;
+  const int64_t* pb_off;   // prefix sums of tiles per pair block, [n_pb + 1]
+  const uint32_t* pb_ij;   // (i, j0) per pair block
+  int64_t n_pb;
+  int64_t n_tiles;
+  int64_t tri;
+  int32_t m, m_pad, w0, w1, n0, n1;
+  unsigned long long* counter;
+  BestSlot* slots;         // one per warp in the grid
+  int32_t top_k;
+  BestSlot* cand;          // [warps][32] when top_k > 1
+  uint32_t* dump_tables;
+  float* dump_scores;
+  int* err;                // set to 1 if a bounded wait expired
+};
+
+// Kernel launchers (scan_int.cu / scan_tc.cu / encode.cu); all asynchronous on `stream`.
 cudaError_t launch_encode(const DevDataset& d, cudaStream_t stream);
 cudaError_t launch_counts(const DevDataset& d, cudaStream_t stream);
 cudaError_t launch_scan_int(const ScanParams& p, int blocks, bool dump, cudaStream_t stream);
@@ -83,6 +105,8 @@ cudaError_t launch_tables(const DevDataset& d, const uint32_t* triplets, int64_t
                           cudaStream_t stream);
 cudaError_t launch_rescore(const DevDataset& d, const BestSlot* cand, int64_t n, Rescored* out, cudaStream_t stream);
 int scan_blocks_per_sm();
+cudaError_t launch_scan_tc(const TcParams& p, int blocks, bool dump, cudaStream_t stream);
+int tc_warps_per_block();
 
 // Host helpers (host_data.cpp).
 void build_k2_lut(int64_t n_max, float* lut);

@@ -1,0 +1,394 @@
+// Tensor-core engine of the triplet search (tcgen05, kind::i8, sm_100a).
+//
+// Same result as the integer engine (scan_int.cu) and as the reference's kernel_epi
+// (GPU/v4.cpp:295-594): the 8 cells of each triplet with g_i, g_j, g_k in {0,1} are
+// counted exactly, the other 19 per class follow by inclusion-exclusion, K2 is scored in
+// the reference's FP32 order, and the lowest (score, i, j, k) wins.
+//
+// Counting as an integer matrix product.  For a fixed SNP i, a block of 32 SNPs j and a
+// block of 128 SNPs k, with 0/1 indicators x_{s,g}(snp) = [genotype of snp in sample s
+// is g]:
+//     D[(j, a, b)][(k, c)] = sum over samples s of class C of
+//                            x_{s,a}(i) * x_{s,b}(j)  *  x_{s,c}(k)
+//                          = count of (g_i=a, g_j=b, g_k=c) in class C.
+// A (128 x S_C) holds the pair indicators of the 32 pairs (i, j) x (a, b), B (256 x S_C)
+// the single indicators of the 128 SNPs k x c; both are expanded from the bit planes to
+// int8 0/1 by the CTA's threads, 128 samples per pipeline stage, straight into shared
+// memory in the no-swizzle K-major layout the tensor core reads (8-row x 16-byte core
+// matrices; K-neighbours 128 B apart, 8-row groups 1024 B apart).  One thread issues
+// tcgen05.mma (M=128, N=256, K=32, int32 accumulators in tensor memory): class 0 into
+// TMEM columns [0,256), class 1 into [256,512).  tcgen05.commit arrives on per-stage
+// mbarriers that release the stage to the producers, and on an accumulator barrier at
+// the end of the tile; the epilogue moves the accumulators TMEM -> registers -> shared
+// memory and completes, scores and selects the 32 x 128 triplets of the tile.
+//
+// Every wait on an mbarrier is bounded (about 2 s of SM clock); on expiry the kernel sets
+// an error word, stops taking tiles, frees its tensor memory and returns.
+#include <cfloat>
+
+#include "epik2_internal.h"
+#include "scan_common.cuh"
+
+namespace epik2 {
+
+constexpr int kTcThreads = 512;  // 16 warps
+constexpr int kTcWarps = kTcThreads / 32;
+constexpr int kTcK = 128;        // SNPs k per tile  -> 256 rows of B
+constexpr int kTcStages = 4;
+constexpr int kStageA = 128 * 128;  // bytes: 128 rows x 128 samples
+constexpr int kStageB = 256 * 128;  // bytes: 256 rows x 128 samples
+constexpr int kStageBytes = kStageA + kStageB;
+constexpr int kTcSmemBytes = kTcStages * kStageBytes + 256;
+constexpr int kEStride = 129;  // words per row of the epilogue staging buffer
+constexpr long long kWaitLimit = 4000000000LL;  // SM clocks (~2 s) before a wait gives up
+// instruction descriptor: D s32, A/B unsigned 8-bit, both K-major, N = 256, M = 128
+constexpr uint32_t kIdescI8 = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+
+// Shared-memory matrix descriptor, no swizzle, K-major: LBO = 128 B (next 16-byte K
+// group), SBO = 1024 B (next group of 8 rows), descriptor version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(kIdescI8), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void bar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the completion of the mbarrier phase with the given parity.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!bar_try_wait(bar, parity)) {
+    if (clock64() - t0 > kWaitLimit) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 16 sample bits -> 16 bytes of 0/1 (byte t = bit t).  Each nibble is spread to the low
+// bit of four bytes by one multiply: x * 0x00204081 places bit t at bit 8t (no carries,
+// the four shifted copies of a 4-bit value do not overlap).
+__device__ __forceinline__ uint4 expand16(uint32_t h) {
+  uint4 r;
+  r.x = ((h & 0xFu) * 0x00204081u) & 0x01010101u;
+  r.y = (((h >> 4) & 0xFu) * 0x00204081u) & 0x01010101u;
+  r.z = (((h >> 8) & 0xFu) * 0x00204081u) & 0x01010101u;
+  r.w = (((h >> 12) & 0xFu) * 0x00204081u) & 0x01010101u;
+  return r;
+}
+
+__device__ __forceinline__ void sts128(uint32_t saddr, uint4 v) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(saddr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+               : "memory");
+}
+
+template <bool kDump, bool kTopK>
+__global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ uint32_t s_tmem;
+  __shared__ long long s_tile;
+  __shared__ int s_abort;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kTcStages * kStageBytes);  // [stages] empty + acc
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t stage0 = smem_u32(smem);
+  const uint32_t bar0 = smem_u32(bars);
+  const uint32_t bar_acc = bar0 + 8 * kTcStages;
+
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; s++) bar_init(bar0 + 8 * s, 1);
+    bar_init(bar_acc, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_abort = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(512u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  const int64_t m_pad = p.m_pad;
+  const int m = p.m;
+  const int64_t tri = p.tri;
+  const int nc0 = (p.w0 + 3) >> 2, nc1 = (p.w1 + 3) >> 2, nct = nc0 + nc1;
+  float best_s = FLT_MAX;
+  unsigned long long best_k = ~0ull;
+  float list_s = FLT_MAX;
+  unsigned long long list_k = ~0ull;
+  uint32_t g_chunk = 0, n_tile = 0;
+  const uint32_t* E = reinterpret_cast<const uint32_t*>(smem);  // epilogue staging, reuses the stages
+
+  for (;;) {
+    if (tid == 0) s_tile = (long long)atomicAdd(p.counter, 1ull);
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile >= p.n_tiles || s_abort) break;
+    int64_t lo = 0, hi = p.n_pb;
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (p.pb_off[mid] <= tile) lo = mid;
+      else hi = mid;
+    }
+    const int i = (int)p.pb_ij[2 * lo], j0 = (int)p.pb_ij[2 * lo + 1];
+    const int k0 = kTcK * ((j0 + 1) / kTcK + (int)(tile - p.pb_off[lo]));
+
+    // ---- producer / MMA pipeline over the class words, 128 samples per stage ----
+    bool aborted = false;
+    for (int cc = 0; cc < nct; ++cc, ++g_chunk) {
+      const int s = (int)(g_chunk % kTcStages);
+      const uint32_t use = g_chunk / kTcStages;
+      bool ok = true;
+      if (use > 0) ok = bar_wait(bar0 + 8 * s, (use & 1u) ^ 1u);
+      if (!ok) s_abort = 1;
+      const int cls = cc < nc0 ? 0 : 1;
+      const int c_in = cls ? cc - nc0 : cc;
+      const int64_t wcls = cls ? p.w1 : p.w0;
+      const int64_t wbase = cls ? p.w0 : 0;
+      const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
+      if (ok) {
+        // A: 128 rows (pair q = r/4, g_i = (r>>1)&1, g_j = r&1) x 8 groups of 16 samples
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int x = tid + kTcThreads * u;
+          const int kg = x >> 7, r = x & 127;
+          const int64_t cw = 4 * c_in + (kg >> 1);
+          uint32_t word = 0;
+          if (cw < wcls) {
+            const uint2* row = p.planes + (wbase + cw) * m_pad;
+            const uint2 gi = __ldg(row + i);
+            const int j = min(j0 + (r >> 2), (int)m_pad - 1);
+            const uint2 gj = __ldg(row + j);
+            word = (((r >> 1) & 1) ? gi.y : gi.x) & ((r & 1) ? gj.y : gj.x);
+          }
+          sts128(sA + (r >> 3) * 1024 + kg * 128 + (r & 7) * 16, expand16((word >> (16 * (kg & 1))) & 0xFFFFu));
+        }
+        // B: 256 rows (k = k0 + n/2, g_k = n&1) x 8 groups of 16 samples
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int x = tid + kTcThreads * u;
+          const int kg = x >> 8, n = x & 255;
+          const int64_t cw = 4 * c_in + (kg >> 1);
+          const int k = k0 + (n >> 1);
+          uint32_t word = 0;
+          if (cw < wcls && k < m_pad) {
+            const uint2 gk = __ldg(p.planes + (wbase + cw) * m_pad + k);
+            word = (n & 1) ? gk.y : gk.x;
+          }
+          sts128(sB + (n >> 3) * 1024 + kg * 128 + (n & 7) * 16, expand16((word >> (16 * (kg & 1))) & 0xFFFFu));
+        }
+      }
+      fence_proxy_async();
+      __syncthreads();
+      if (s_abort) {
+        aborted = true;
+        break;
+      }
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(cls * 256);
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++)
+          mma_i8(d, smem_desc(sA + kk * 256), smem_desc(sB + kk * 256), (c_in > 0 || kk > 0) ? 1u : 0u);
+        mma_commit(bar0 + 8 * s);
+        if (cc == nct - 1) mma_commit(bar_acc);
+      }
+    }
+    if (aborted) break;
+
+    // ---- epilogue: TMEM -> shared -> complete tables, score, select ----
+    {
+      const bool ok = bar_wait(bar_acc, n_tile & 1u);
+      if (!ok) s_abort = 1;
+      __syncthreads();
+      if (s_abort) break;
+    }
+    tc_fence_after();
+    ++n_tile;
+    const int quarter = warp & 3, cgrp = warp >> 2;  // TMEM lanes 32*quarter.., columns 32*cgrp.. of a half
+    const int row = 32 * quarter + lane;
+    const uint2 si0 = *reinterpret_cast<const uint2*>(p.singles + ((int64_t)i) * 2);
+    const uint2 si1 = *reinterpret_cast<const uint2*>(p.singles + (m_pad + i) * 2);
+    for (int h = 0; h < 2; h++) {
+      uint32_t* Ew = reinterpret_cast<uint32_t*>(smem);
+#pragma unroll
+      for (int cls = 0; cls < 2; cls++) {
+        const bool has = cls ? nc1 > 0 : nc0 > 0;
+#pragma unroll
+        for (int part = 0; part < 2; part++) {
+          const int col = 128 * h + 32 * cgrp + 16 * part;  // column inside the class accumulator
+          uint32_t v[16];
+          if (has) {
+            tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(cls * 256 + col), v);
+            tmem_wait_ld();
+          } else {
+#pragma unroll
+            for (int t = 0; t < 16; t++) v[t] = 0;
+          }
+          uint32_t* dst = Ew + (cls * 128 + row) * kEStride + (col - 128 * h);
+#pragma unroll
+          for (int t = 0; t < 16; t++) dst[t] = v[t];
+        }
+      }
+      tc_fence_before();
+      __syncthreads();
+      // 32 pairs x 64 k of this half; thread -> pair q, k = 16u + (tid & 15)
+      const int q = tid >> 4;
+      const int j = j0 + q;
+#pragma unroll 1
+      for (int u = 0; u < 4; u++) {
+        const int kl = 16 * u + (tid & 15);
+        const int k = k0 + 64 * h + kl;
+        const bool valid = (j < m) && (k > j) && (k < m);
+        float sc = FLT_MAX;
+        unsigned long long key = ~0ull;
+        if (valid) {
+          uint32_t t80[8], t81[8];
+#pragma unroll
+          for (int ab = 0; ab < 4; ab++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+              t80[2 * ab + c] = E[(0 * 128 + 4 * q + ab) * kEStride + 2 * kl + c];
+              t81[2 * ab + c] = E[(1 * 128 + 4 * q + ab) * kEStride + 2 * kl + c];
+            }
+          const uint2 sj0 = *reinterpret_cast<const uint2*>(p.singles + ((int64_t)j) * 2);
+          const uint2 sj1 = *reinterpret_cast<const uint2*>(p.singles + (m_pad + j) * 2);
+          const uint2 sk0 = *reinterpret_cast<const uint2*>(p.singles + ((int64_t)k) * 2);
+          const uint2 sk1 = *reinterpret_cast<const uint2*>(p.singles + (m_pad + k) * 2);
+          const int64_t oij = tri_offset(m_pad, i, j), oik = tri_offset(m_pad, i, k), ojk = tri_offset(m_pad, j, k);
+          const uint4 pij0 = __ldg(p.pairs + oij), pij1 = __ldg(p.pairs + tri + oij);
+          const uint4 pik0 = __ldg(p.pairs + oik), pik1 = __ldg(p.pairs + tri + oik);
+          const uint4 pjk0 = __ldg(p.pairs + ojk), pjk1 = __ldg(p.pairs + tri + ojk);
+          uint32_t T0[27], T1[27];
+          complete_table(t80, (uint32_t)p.n0, si0, sj0, sk0, pij0, pik0, pjk0, T0);
+          complete_table(t81, (uint32_t)p.n1, si1, sj1, sk1, pij1, pik1, pjk1, T1);
+          sc = k2_score(T0, T1, p.lut);
+          key = pack_key((uint64_t)i, (uint64_t)j, (uint64_t)k);
+          if (kDump) {
+            const int64_t t = triplet_index(m, i, j, k);
+            uint32_t* dt = p.dump_tables + t * 54;
+#pragma unroll
+            for (int c = 0; c < 27; c++) {
+              dt[c] = T0[c];
+              dt[27 + c] = T1[c];
+            }
+            p.dump_scores[t] = sc;
+          }
+          if (better(sc, key, best_s, best_k)) {
+            best_s = sc;
+            best_k = key;
+          }
+        }
+        if (kTopK) {
+          const float ts = __shfl_sync(kFull, list_s, 31);
+          const unsigned long long tk = __shfl_sync(kFull, list_k, 31);
+          unsigned want = __ballot_sync(kFull, valid && better(sc, key, ts, tk));
+          while (want) {
+            const int src = __ffs(want) - 1;
+            want &= want - 1;
+            const float cs = __shfl_sync(kFull, sc, src);
+            const unsigned long long ck = __shfl_sync(kFull, key, src);
+            const float ts2 = __shfl_sync(kFull, list_s, 31);
+            const unsigned long long tk2 = __shfl_sync(kFull, list_k, 31);
+            if (better(cs, ck, ts2, tk2)) warp_list_insert(list_s, list_k, cs, ck, lane);
+          }
+        }
+      }
+      __syncthreads();  // the staging buffer is rewritten by the next half / next tile
+    }
+  }
+
+  // ---- teardown: every MMA has completed (its tile's accumulator barrier was waited) ----
+  tc_fence_before();
+  __syncthreads();
+  if (s_abort && tid == 0) atomicExch(p.err, 1);
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const float os = __shfl_xor_sync(kFull, best_s, off);
+    const unsigned long long ok = __shfl_xor_sync(kFull, best_k, off);
+    if (better(os, ok, best_s, best_k)) {
+      best_s = os;
+      best_k = ok;
+    }
+  }
+  const int64_t gwarp = (int64_t)blockIdx.x * kTcWarps + warp;
+  if (lane == 0) {
+    p.slots[gwarp].score = best_s;
+    p.slots[gwarp].key = best_k;
+  }
+  if (kTopK) {
+    p.cand[gwarp * 32 + lane].score = list_s;
+    p.cand[gwarp * 32 + lane].key = list_k;
+  }
+}
+
+int tc_warps_per_block() { return kTcWarps; }
+
+cudaError_t launch_scan_tc(const TcParams& p, int blocks, bool dump, cudaStream_t stream) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_scan_tc<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kTcSmemBytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_scan_tc<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_scan_tc<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const bool topk = p.top_k > 1;
+  if (dump) k_scan_tc<true, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+  else if (topk) k_scan_tc<false, true><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+  else k_scan_tc<false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace epik2

@@ -29,6 +29,10 @@ E_NO_DEVICE = -7
 E_BUSY = -8
 E_CANCELLED = -9
 
+ENGINE_AUTO = 0
+ENGINE_INT = 1
+ENGINE_TC = 2
+
 
 class Epik2Error(RuntimeError):
     def __init__(self, status, msg):
@@ -114,6 +118,7 @@ def library():
         "epik2_get_stats": ([p, ctypes.POINTER(Stats)], ctypes.c_int),
         "epik2_reset_stats": ([p], ctypes.c_int),
         "epik2_scan_u8_noalloc": ([p, p, i64, i64, p, ctypes.POINTER(Best)], ctypes.c_int),
+        "epik2_set_engine": ([p, ctypes.c_int], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -193,13 +198,15 @@ def n_triplets(m):
 class Context:
     """One device context: owns a CUDA stream and the resident datasets."""
 
-    def __init__(self, device=0):
+    def __init__(self, device=0, engine=ENGINE_AUTO):
         self._lib = library()
         h = ctypes.c_void_p()
         r = self._lib.epik2_create(ctypes.byref(h), device)
         if r:
             raise Epik2Error(r, strerror(r))
         self._h = h
+        if engine:
+            self.set_engine(engine)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -226,6 +233,10 @@ class Context:
     @property
     def handle(self):
         return self._h
+
+    def set_engine(self, engine):
+        """Default engine of this context: ENGINE_AUTO, ENGINE_INT or ENGINE_TC."""
+        self._check(self._lib.epik2_set_engine(self._h, engine))
 
     def stats(self):
         st = Stats()

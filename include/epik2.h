@@ -69,7 +69,7 @@ typedef struct {
 
 /* Scan options.  Zero-initialise and set what you need; 0 means "default". */
 typedef struct {
-  int32_t engine;      /* 0 = default (fastest available), 1 = integer-pipe kernel */
+  int32_t engine;      /* 0 = the context's default, 1 = integer pipe (LOP3+POPC), 2 = tensor cores */
   int32_t top_k;       /* 0/1 = best only; >1 = keep the top_k lowest FP32 scores */
   int32_t rescore_fp64;/* 1 = rescore the kept candidates in FP64 on the GPU */
   int32_t k_strip;     /* tuning: SNPs per k-strip (multiple of 32); 0 = autotuned */
@@ -90,6 +90,13 @@ const char *epik2_last_error(const epik2_ctx *ctx);
 int epik2_device_name(const epik2_ctx *ctx, char *buf, size_t len);
 /* Bytes of device memory currently free / total on the context's device. */
 int epik2_mem_info(const epik2_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
+
+/* Default search engine of the context (EPIK2_ENGINE_*).  Both engines give identical
+ * tables, scores and triplets; AUTO is the tensor-core engine. */
+#define EPIK2_ENGINE_AUTO 0
+#define EPIK2_ENGINE_INT 1 /* integer pipe: 8 LOP3+POPC per triplet and 32-sample word */
+#define EPIK2_ENGINE_TC 2  /* tcgen05 int8 matrix products on 0/1 operands, int32 accumulators */
+int epik2_set_engine(epik2_ctx *ctx, int engine);
 
 /* Run the context's work on a caller-owned stream (e.g. a PyTorch stream); NULL restores
  * the context's own stream.  The library still synchronises that stream before it

@@ -56,10 +56,14 @@ def pytest_collection_modifyitems(config, items):
             item.add_marker(skip)
 
 
-@pytest.fixture(scope="session")
-def ctx():
+ENGINES = {1: "int", 2: "tc"}
+
+
+@pytest.fixture(scope="session", params=[1, 2], ids=["int", "tc"])
+def ctx(request):
+    """A device context per search engine: every test that takes `ctx` runs on both."""
     import epik2
-    c = epik2.Context(0)
+    c = epik2.Context(0, engine=request.param)
     yield c
     c.close()
 
