@@ -178,8 +178,37 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
     const int k0 = kTcK * ((j0 + 1) / kTcK + (int)(tile - p.pb_off[lo]));
 
     // ---- producer / MMA pipeline over the class words, 128 samples per stage ----
+    // Thread roles in a stage (4 class words = 128 samples):
+    //   A row r = 32*ab + q (pair q, g_i = ab>>1, g_j = ab&1), word w: ab = tid>>7,
+    //     w = (tid>>5)&3, q = lane -> one warp writes 32 consecutive rows;
+    //   B row n = 128*c + kl (k = k0+kl, g_k = c), word w: kl = tid&127, w = tid>>7.
+    // The words of stage cc+1 are loaded while stage cc is expanded.
+    const int a_ab = tid >> 7, a_w = (tid >> 5) & 3, a_q = lane;
+    const int a_row = 32 * a_ab + a_q;
+    const int a_j = min(j0 + a_q, (int)m_pad - 1);
+    const int b_kl = tid & 127, b_w = tid >> 7;
+    const int b_k = k0 + b_kl;
+    auto load_words = [&](int cc, uint2& gi, uint2& gj, uint2& gk) {
+      const int cls = cc < nc0 ? 0 : 1;
+      const int c_in = cls ? cc - nc0 : cc;
+      const int64_t wcls = cls ? p.w1 : p.w0;
+      const int64_t wbase = (cls ? p.w0 : 0) + 4 * c_in;
+      gi = make_uint2(0, 0);
+      gj = make_uint2(0, 0);
+      gk = make_uint2(0, 0);
+      if (4 * c_in + a_w < wcls) {
+        const uint2* row = p.planes + (wbase + a_w) * m_pad;
+        gi = __ldg(row + i);
+        gj = __ldg(row + a_j);
+      }
+      if (4 * c_in + b_w < wcls && b_k < m_pad) gk = __ldg(p.planes + (wbase + b_w) * m_pad + b_k);
+    };
+    uint2 ci, cj, ck;
+    if (nct > 0) load_words(0, ci, cj, ck);
     bool aborted = false;
     for (int cc = 0; cc < nct; ++cc, ++g_chunk) {
+      uint2 ni = make_uint2(0, 0), nj = ni, nk = ni;
+      if (cc + 1 < nct) load_words(cc + 1, ni, nj, nk);
       const int s = (int)(g_chunk % kTcStages);
       const uint32_t use = g_chunk / kTcStages;
       bool ok = true;
@@ -187,41 +216,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
       if (!ok) s_abort = 1;
       const int cls = cc < nc0 ? 0 : 1;
       const int c_in = cls ? cc - nc0 : cc;
-      const int64_t wcls = cls ? p.w1 : p.w0;
-      const int64_t wbase = cls ? p.w0 : 0;
       const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
       if (ok) {
-        // A: 128 rows (pair q = r/4, g_i = (r>>1)&1, g_j = r&1) x 8 groups of 16 samples
+        const uint32_t wa = ((a_ab >> 1) ? ci.y : ci.x) & ((a_ab & 1) ? cj.y : cj.x);
+        const uint32_t offa = sA + (a_row >> 3) * 1024 + (a_row & 7) * 16 + (2 * a_w) * 128;
+        sts128(offa, expand16(wa & 0xFFFFu));
+        sts128(offa + 128, expand16(wa >> 16));
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-          const int x = tid + kTcThreads * u;
-          const int kg = x >> 7, r = x & 127;
-          const int64_t cw = 4 * c_in + (kg >> 1);
-          uint32_t word = 0;
-          if (cw < wcls) {
-            const uint2* row = p.planes + (wbase + cw) * m_pad;
-            const uint2 gi = __ldg(row + i);
-            const int j = min(j0 + (r >> 2), (int)m_pad - 1);
-            const uint2 gj = __ldg(row + j);
-            word = (((r >> 1) & 1) ? gi.y : gi.x) & ((r & 1) ? gj.y : gj.x);
-          }
-          sts128(sA + (r >> 3) * 1024 + kg * 128 + (r & 7) * 16, expand16((word >> (16 * (kg & 1))) & 0xFFFFu));
-        }
-        // B: 256 rows (k = k0 + n/2, g_k = n&1) x 8 groups of 16 samples
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int x = tid + kTcThreads * u;
-          const int kg = x >> 8, n = x & 255;
-          const int64_t cw = 4 * c_in + (kg >> 1);
-          const int k = k0 + (n >> 1);
-          uint32_t word = 0;
-          if (cw < wcls && k < m_pad) {
-            const uint2 gk = __ldg(p.planes + (wbase + cw) * m_pad + k);
-            word = (n & 1) ? gk.y : gk.x;
-          }
-          sts128(sB + (n >> 3) * 1024 + kg * 128 + (n & 7) * 16, expand16((word >> (16 * (kg & 1))) & 0xFFFFu));
+        for (int c = 0; c < 2; c++) {
+          const int n = 128 * c + b_kl;
+          const uint32_t wb = c ? ck.y : ck.x;
+          const uint32_t offb = sB + (n >> 3) * 1024 + (n & 7) * 16 + (2 * b_w) * 128;
+          sts128(offb, expand16(wb & 0xFFFFu));
+          sts128(offb + 128, expand16(wb >> 16));
         }
       }
+      ci = ni;
+      cj = nj;
+      ck = nk;
       fence_proxy_async();
       __syncthreads();
       if (s_abort) {
@@ -249,8 +261,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
     }
     tc_fence_after();
     ++n_tile;
-    const int quarter = warp & 3, cgrp = warp >> 2;  // TMEM lanes 32*quarter.., columns 32*cgrp.. of a half
+    // Accumulator layout: TMEM lane = 32*ab + q, column = 128*c + kl (per class: +256*cls).
+    // Per half h (kl in [64h, 64h+64)) each warp copies lanes 32*(warp&3).. and 32 columns
+    // of both c into E[cls][lane][64*c + kl - 64h] (row stride kEStride words).
+    const int quarter = warp & 3, cgrp = warp >> 2;
     const int row = 32 * quarter + lane;
+    const int e_c = cgrp >> 1, e_sub = cgrp & 1;
     const uint2 si0 = *reinterpret_cast<const uint2*>(p.singles + ((int64_t)i) * 2);
     const uint2 si1 = *reinterpret_cast<const uint2*>(p.singles + (m_pad + i) * 2);
     for (int h = 0; h < 2; h++) {
@@ -260,7 +276,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
         const bool has = cls ? nc1 > 0 : nc0 > 0;
 #pragma unroll
         for (int part = 0; part < 2; part++) {
-          const int col = 128 * h + 32 * cgrp + 16 * part;  // column inside the class accumulator
+          const int col = 128 * e_c + 64 * h + 32 * e_sub + 16 * part;  // inside the class accumulator
           uint32_t v[16];
           if (has) {
             tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(cls * 256 + col), v);
@@ -269,19 +285,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
 #pragma unroll
             for (int t = 0; t < 16; t++) v[t] = 0;
           }
-          uint32_t* dst = Ew + (cls * 128 + row) * kEStride + (col - 128 * h);
+          uint32_t* dst = Ew + (cls * 128 + row) * kEStride + 64 * e_c + 32 * e_sub + 16 * part;
 #pragma unroll
           for (int t = 0; t < 16; t++) dst[t] = v[t];
         }
       }
       tc_fence_before();
       __syncthreads();
-      // 32 pairs x 64 k of this half; thread -> pair q, k = 16u + (tid & 15)
-      const int q = tid >> 4;
-      const int j = j0 + q;
+      // 32 pairs x 64 k of this half: triplet x = tid + 512u -> kl = x & 63, q = x >> 6
 #pragma unroll 1
       for (int u = 0; u < 4; u++) {
-        const int kl = 16 * u + (tid & 15);
+        const int x = tid + kTcThreads * u;
+        const int kl = x & 63, q = x >> 6;
+        const int j = j0 + q;
         const int k = k0 + 64 * h + kl;
         const bool valid = (j < m) && (k > j) && (k < m);
         float sc = FLT_MAX;
@@ -292,8 +308,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
           for (int ab = 0; ab < 4; ab++)
 #pragma unroll
             for (int c = 0; c < 2; c++) {
-              t80[2 * ab + c] = E[(0 * 128 + 4 * q + ab) * kEStride + 2 * kl + c];
-              t81[2 * ab + c] = E[(1 * 128 + 4 * q + ab) * kEStride + 2 * kl + c];
+              t80[2 * ab + c] = E[(0 * 128 + 32 * ab + q) * kEStride + 64 * c + kl];
+              t81[2 * ab + c] = E[(1 * 128 + 32 * ab + q) * kEStride + 64 * c + kl];
             }
           const uint2 sj0 = *reinterpret_cast<const uint2*>(p.singles + ((int64_t)j) * 2);
           const uint2 sj1 = *reinterpret_cast<const uint2*>(p.singles + (m_pad + j) * 2);
