@@ -13,7 +13,7 @@
 //                          = count of (g_i=a, g_j=b, g_k=c) in class C.
 // A (128 x S_C) holds the pair indicators of the 32 pairs (i, j) x (a, b), B (256 x S_C)
 // the single indicators of the 128 SNPs k x c; both are expanded from the bit planes to
-// int8 0/1 by the CTA's threads, 128 samples per pipeline stage, straight into shared
+// int8 (0 or -1) by the CTA's threads, 128 samples per pipeline stage, straight into shared
 // memory in the no-swizzle K-major layout the tensor core reads (8-row x 16-byte core
 // matrices; K-neighbours 128 B apart, 8-row groups 1024 B apart).  One thread issues
 // tcgen05.mma (M=128, N=256, K=32, int32 accumulators in tensor memory): class 0 into
@@ -41,8 +41,8 @@ constexpr int kStageBytes = kStageA + kStageB;
 constexpr int kTcSmemBytes = kTcStages * kStageBytes + 256;
 constexpr int kEStride = 129;  // words per row of the epilogue staging buffer
 constexpr long long kWaitLimit = 4000000000LL;  // SM clocks (~2 s) before a wait gives up
-// instruction descriptor: D s32, A/B unsigned 8-bit, both K-major, N = 256, M = 128
-constexpr uint32_t kIdescI8 = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+// instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = 256, M = 128
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
   return (uint32_t)__cvta_generic_to_shared(ptr);
@@ -106,15 +106,26 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// 16 sample bits -> 16 bytes of 0/1 (byte t = bit t).  Each nibble is spread to the low
-// bit of four bytes by one multiply: x * 0x00204081 places bit t at bit 8t (no carries,
-// the four shifted copies of a 4-bit value do not overlap).
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+  return d;
+}
+
+// 16 sample bits (low half of h) -> 16 int8 operand bytes, 0 (absent) or -1 (present);
+// both operands use -1, so every product is 0 or (-1)*(-1) = +1 and the int32 sums are
+// the exact counts.  One PRMT per 4 bytes: the selector is h itself, whose nibble b holds
+// sample bits 4b..4b+3; the 8-byte pools alternate 0x00/0xFF so that the byte picked by
+// the nibble's low 3 bits is 0xFF exactly when the tested bit (bit 0, 1 or 2 of the
+// nibble) is set, and the nibble's sign-replicate bit cannot change a 0x00/0xFF byte.
+// Byte 4t+b of the group therefore holds sample t+4b: the same sample order is used for
+// A and B, so the products still pair each sample with itself.
 __device__ __forceinline__ uint4 expand16(uint32_t h) {
   uint4 r;
-  r.x = ((h & 0xFu) * 0x00204081u) & 0x01010101u;
-  r.y = (((h >> 4) & 0xFu) * 0x00204081u) & 0x01010101u;
-  r.z = (((h >> 8) & 0xFu) * 0x00204081u) & 0x01010101u;
-  r.w = (((h >> 12) & 0xFu) * 0x00204081u) & 0x01010101u;
+  r.x = prmt(0xFF00FF00u, 0xFF00FF00u, h);        // nibble bit 0: samples 0, 4, 8, 12
+  r.y = prmt(0xFFFF0000u, 0xFFFF0000u, h);        // nibble bit 1: samples 1, 5, 9, 13
+  r.z = prmt(0x00000000u, 0xFFFFFFFFu, h);        // nibble bit 2: samples 2, 6, 10, 14
+  r.w = prmt(0xFF00FF00u, 0xFF00FF00u, h >> 3);   // nibble bit 3 via shift: 3, 7, 11, 15
   return r;
 }
 
@@ -220,14 +231,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
       if (ok) {
         const uint32_t wa = ((a_ab >> 1) ? ci.y : ci.x) & ((a_ab & 1) ? cj.y : cj.x);
         const uint32_t offa = sA + (a_row >> 3) * 1024 + (a_row & 7) * 16 + (2 * a_w) * 128;
-        sts128(offa, expand16(wa & 0xFFFFu));
+        sts128(offa, expand16(wa));
         sts128(offa + 128, expand16(wa >> 16));
 #pragma unroll
         for (int c = 0; c < 2; c++) {
           const int n = 128 * c + b_kl;
           const uint32_t wb = c ? ck.y : ck.x;
           const uint32_t offb = sB + (n >> 3) * 1024 + (n & 7) * 16 + (2 * b_w) * 128;
-          sts128(offb, expand16(wb & 0xFFFFu));
+          sts128(offb, expand16(wb));
           sts128(offb + 128, expand16(wb >> 16));
         }
       }
