@@ -44,6 +44,40 @@ struct epik2_ctx {
   BestSlot* h_best = nullptr;   // pinned
   // last top-k result
   std::vector<epik2_best> last_topk;
+  // autotuner choices per (log2 samples, log2 SNPs)
+  std::map<std::pair<int, int>, epik2_tune> tune_cache;
+  // batched-form plans, keyed by the dataset ids
+  std::map<std::vector<int32_t>, std::unique_ptr<struct BatchPlan>> plans;
+};
+
+struct BatchPlan {
+  int kw = 4;
+  int64_t n_tiles = 0;
+  int32_t n_jobs = 0;
+  epik2::TcJob* d_jobs = nullptr;
+  int64_t* d_job_off = nullptr;
+  int64_t* d_pb_off = nullptr;
+  uint32_t* d_pb_ij = nullptr;
+  epik2::BestSlot* d_job_slots = nullptr;
+  epik2::BestSlot* d_results = nullptr;
+  epik2::BestSlot* h_results = nullptr;  // pinned
+  int* h_err = nullptr;                  // pinned
+  std::vector<epik2::TcJob> h_jobs;
+  std::vector<int64_t> pb_base;          // offset of each job's pair-block list
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~BatchPlan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaFree(d_jobs);
+    cudaFree(d_job_off);
+    cudaFree(d_pb_off);
+    cudaFree(d_pb_ij);
+    cudaFree(d_job_slots);
+    cudaFree(d_results);
+    cudaFreeHost(h_results);
+    cudaFreeHost(h_err);
+  }
 };
 
 namespace {
@@ -158,7 +192,10 @@ int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
 
 int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_k, int n_warps);
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
-                float* dump_scores, BestSlot* best_out, const epik2_opts* opts);
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw);
+int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out);
+int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* dump_tables, float* dump_scores,
+             BestSlot* best_out);
 
 // Pair groups of first index i: j0 = i+1, i+5, ... while j0 <= m-2.
 int64_t groups_of(int64_t m, int64_t i) { return (i <= m - 3) ? (m - 2 - i + kPairsPerWarp) / kPairsPerWarp : 0; }
@@ -180,8 +217,16 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   if (ie < ib) ie = ib;
   int engine = ctx->engine;
   if (opts && opts->engine != 0) engine = opts->engine;
-  if (engine == 0) engine = 2;
-  if (engine == 2) return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts);
+  int kw = (opts && opts->stage_words) ? opts->stage_words : 0;
+  if (kw != 0 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
+  if (engine == 0 || (engine == 2 && kw == 0)) {
+    epik2_tune t{};
+    int r = tuned(ctx, d, &t);
+    if (r) return r;
+    if (engine == 0) engine = t.engine;
+    if (kw == 0) kw = t.stage_words;
+  }
+  if (engine == 2) return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts, kw);
   const int64_t n_first = std::max<int64_t>(ie - ib, 1);
   std::vector<int64_t> off((size_t)n_first + 1, 0);
   for (int64_t t = 0; t < n_first; t++) off[(size_t)t + 1] = off[(size_t)t] + (ib + t < ie ? groups_of(m, ib + t) : 0);
@@ -289,7 +334,7 @@ int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_
 
 // Tensor-core engine: one CTA per SM, tiles = pair blocks (i, j0..j0+31) x k blocks of 128.
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
-                float* dump_scores, BestSlot* best_out, const epik2_opts* opts) {
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw) {
   const int64_t m = d.n_snps;
   const int64_t n_kb = (m + 127) / 128;
   std::vector<uint32_t> ij;
@@ -336,7 +381,7 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   p.dump_scores = dump_scores;
   p.err = ctx->d_err;
   CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
-  CK(ctx, launch_scan_tc(p, ctx->tc_blocks, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
+  CK(ctx, launch_scan_tc(p, ctx->tc_blocks, kw, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
   CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
   const int n_warps = ctx->tc_blocks * tc_warps_per_block();
   CK(ctx, launch_reduce_best(ctx->d_slots, n_warps, ctx->d_best, ctx->stream), "reduce kernel");
@@ -360,6 +405,196 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   ctx->stats.last_scan_words = d.w0 + d.w1;
   *best_out = *ctx->h_best;
   return collect_topk(ctx, d, opts, top_k, n_warps);
+}
+
+// Triplets with first index in [0, ie).
+int64_t triplets_before(int64_t m, int64_t ie) {
+  int64_t t = 0;
+  for (int64_t i = 0; i < ie; i++) t += (m - 1 - i) * (m - 2 - i) / 2;
+  return t;
+}
+
+// Autotuner: time each candidate on a slice of the dataset (first indices [0, ie) holding
+// about 1/64 of the triplets, grown until the tensor-core engine has >= 4 tiles per SM)
+// and keep the fastest per shape bucket.  Each candidate runs twice; the second run is
+// timed (the first absorbs first-launch costs).
+int autotune_now(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
+  const int64_t m = d.n_snps, total = triplets_before(m, m);
+  int64_t ie = 1;
+  while (ie < m && (triplets_before(m, ie) * 64 < total || triplets_before(m, ie) < 4ll * ctx->tc_blocks * 4096)) ie++;
+  const double ts = (double)triplets_before(m, ie) * (double)d.n_samples;
+  double rate[3] = {0, 0, 0};
+  const int eng[3] = {1, 2, 2}, kws[3] = {0, 4, 8};
+  for (int c = 0; c < 3; c++) {
+    epik2_opts o{};
+    o.engine = eng[c];
+    o.stage_words = kws[c];
+    o.snp_begin = 0;
+    o.snp_end = ie;
+    BestSlot b{};
+    for (int rep = 0; rep < 2; rep++) {
+      int r = run_scan(ctx, d, &o, nullptr, nullptr, &b);
+      if (r) return r;
+    }
+    rate[c] = ts / (ctx->stats.last_scan_kernel_ms * 1e-3);
+  }
+  epik2_tune t{};
+  t.rate_int = rate[0];
+  t.rate_tc4 = rate[1];
+  t.rate_tc8 = rate[2];
+  t.stage_words = rate[2] > rate[1] ? 8 : 4;
+  t.engine = std::max(rate[1], rate[2]) >= rate[0] ? 2 : 1;
+  *out = t;
+  return EPIK2_OK;
+}
+
+std::pair<int, int> shape_bucket(const DevDataset& d) {
+  int sb = 0, mb = 0;
+  while ((2ll << sb) <= d.n_samples) sb++;
+  while ((2ll << mb) <= d.n_snps) mb++;
+  return {sb, mb};
+}
+
+int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
+  const auto key = shape_bucket(d);
+  auto it = ctx->tune_cache.find(key);
+  if (it != ctx->tune_cache.end()) {
+    *out = it->second;
+    return EPIK2_OK;
+  }
+  int r = autotune_now(ctx, d, out);
+  if (r) return r;
+  ctx->tune_cache[key] = *out;
+  return EPIK2_OK;
+}
+
+// Batched form: build (or reuse) the plan for these datasets, refresh the job table from
+// the datasets' current class split, replay the captured launch sequence.
+int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vector<int32_t>& ids, int kw,
+              epik2_best* out) {
+  std::vector<int32_t> key = ids;
+  key.push_back(kw);
+  BatchPlan* plan = nullptr;
+  auto it = ctx->plans.find(key);
+  const int32_t n = (int32_t)ds.size();
+  const int grid = ctx->tc_blocks;
+  if (it != ctx->plans.end()) {
+    plan = it->second.get();
+  } else {
+    std::unique_ptr<BatchPlan> pl(new BatchPlan());
+    pl->kw = kw;
+    pl->n_jobs = n;
+    std::vector<int64_t> job_off(1, 0), pb_off_all;
+    std::vector<uint32_t> pb_ij_all;
+    for (int32_t b = 0; b < n; b++) {
+      const int64_t m = ds[b]->n_snps, n_kb = (m + 127) / 128;
+      pl->pb_base.push_back((int64_t)pb_off_all.size());
+      int64_t tiles = 0;
+      pb_off_all.push_back(0);
+      int64_t n_pb = 0;
+      for (int64_t i = 0; i < m; i++)
+        for (int64_t j0 = i + 1; j0 <= m - 2; j0 += 32) {
+          pb_ij_all.push_back((uint32_t)i);
+          pb_ij_all.push_back((uint32_t)j0);
+          tiles += n_kb - (j0 + 1) / 128;
+          pb_off_all.push_back(tiles);
+          n_pb++;
+        }
+      job_off.push_back(job_off.back() + tiles);
+      TcJob j{};
+      j.n_pb = std::max<int64_t>(n_pb, 1);
+      pl->h_jobs.push_back(j);
+    }
+    pl->n_tiles = job_off.back();
+    const size_t pb_ij_bytes = std::max<size_t>(pb_ij_all.size(), 2) * 4;
+    if (cudaMalloc(&pl->d_jobs, sizeof(TcJob) * n) || cudaMalloc(&pl->d_job_off, 8 * (n + 1)) ||
+        cudaMalloc(&pl->d_pb_off, 8 * pb_off_all.size()) || cudaMalloc(&pl->d_pb_ij, pb_ij_bytes) ||
+        cudaMalloc(&pl->d_job_slots, sizeof(BestSlot) * (size_t)n * grid) ||
+        cudaMalloc(&pl->d_results, sizeof(BestSlot) * n) || cudaMallocHost(&pl->h_results, sizeof(BestSlot) * n) ||
+        cudaMallocHost(&pl->h_err, sizeof(int)))
+      return fail(ctx, EPIK2_E_NOMEM, "batched plan: device memory");
+    CK(ctx, cudaMemcpyAsync(pl->d_job_off, job_off.data(), 8 * (n + 1), cudaMemcpyHostToDevice, ctx->stream),
+       "upload batch");
+    CK(ctx, cudaMemcpyAsync(pl->d_pb_off, pb_off_all.data(), 8 * pb_off_all.size(), cudaMemcpyHostToDevice,
+                            ctx->stream),
+       "upload batch");
+    if (!pb_ij_all.empty())
+      CK(ctx, cudaMemcpyAsync(pl->d_pb_ij, pb_ij_all.data(), 4 * pb_ij_all.size(), cudaMemcpyHostToDevice,
+                              ctx->stream),
+         "upload batch");
+    ctx->stats.h2d_bytes += 8 * (n + 1) + 8 * pb_off_all.size() + 4 * pb_ij_all.size();
+    CK(ctx, cudaStreamSynchronize(ctx->stream), "upload batch");
+    // capture: reset slots, counter and error word; batched search; per-dataset reduce; read back
+    TcParams p{};
+    p.counter = ctx->d_counter;
+    p.err = ctx->d_err;
+    p.jobs = pl->d_jobs;
+    p.job_tile_off = pl->d_job_off;
+    p.n_jobs = n;
+    p.job_slots = pl->d_job_slots;
+    p.n_tiles = pl->n_tiles;
+    p.n_pb = 1;
+    CK(ctx, tc_configure(), "configure");
+    CK(ctx, launch_fill_slots(pl->d_job_slots, (int64_t)n * grid, ctx->stream), "configure");  // also loads modules
+    CK(ctx, cudaStreamSynchronize(ctx->stream), "configure");
+    CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+    cudaError_t e = launch_fill_slots(pl->d_job_slots, (int64_t)n * grid, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream);
+    if (e == cudaSuccess) e = launch_scan_tc(p, grid, kw, false, ctx->stream);
+    if (e == cudaSuccess) e = launch_reduce_jobs(pl->d_job_slots, n, grid, pl->d_results, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(pl->h_results, pl->d_results, sizeof(BestSlot) * n, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(pl->h_err, ctx->d_err, 4, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &pl->graph);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&pl->exec, pl->graph, 0);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batched graph");
+    plan = pl.get();
+    ctx->plans[key] = std::move(pl);
+  }
+  // refresh the job table (class splits may have changed since the plan was built)
+  for (int32_t b = 0; b < n; b++) {
+    const DevDataset& d = *ds[b];
+    TcJob& j = plan->h_jobs[b];
+    j.planes = d.planes;
+    j.singles = d.singles;
+    j.pairs = d.pairs;
+    j.lut = d.lut;
+    j.pb_off = plan->d_pb_off + plan->pb_base[b];
+    j.pb_ij = plan->d_pb_ij + 2 * (plan->pb_base[b] - b);
+    j.tri = d.tri;
+    j.m = (int32_t)d.n_snps;
+    j.m_pad = (int32_t)d.m_pad;
+    j.w0 = (int32_t)d.w0;
+    j.w1 = (int32_t)d.w1;
+    j.n0 = (int32_t)d.n_controls;
+    j.n1 = (int32_t)d.n_cases;
+  }
+  CK(ctx, cudaMemcpyAsync(plan->d_jobs, plan->h_jobs.data(), sizeof(TcJob) * n, cudaMemcpyHostToDevice, ctx->stream),
+     "upload job table");
+  ctx->stats.h2d_bytes += sizeof(TcJob) * n;
+  CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
+  CK(ctx, cudaGraphLaunch(plan->exec, ctx->stream), "batched graph launch");
+  CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
+  CK(ctx, cudaStreamSynchronize(ctx->stream), "batched search");
+  ctx->stats.kernel_launches += 3;
+  ctx->stats.d2h_bytes += sizeof(BestSlot) * n + 4;
+  if (*plan->h_err) return fail(ctx, EPIK2_E_TIMEOUT, "batched search: a bounded wait expired");
+  float kms = 0.0f;
+  CK(ctx, cudaEventElapsedTime(&kms, ctx->ev_start, ctx->ev_stop), "event time");
+  ctx->stats.last_scan_kernel_ms = kms;
+  int64_t trip = 0;
+  for (auto* d : ds) trip += triplets_before(d->n_snps, d->n_snps);
+  ctx->stats.last_scan_triplets = trip;
+  ctx->stats.last_scan_words = 0;
+  for (int32_t b = 0; b < n; b++) {
+    const BestSlot& r = plan->h_results[b];
+    out[b].score = r.score;
+    out[b].score_fp64 = std::numeric_limits<double>::quiet_NaN();
+    decode_key(r.key, out[b].i, out[b].j, out[b].k);
+  }
+  return EPIK2_OK;
 }
 
 }  // namespace
@@ -420,6 +655,7 @@ void epik2_destroy(epik2_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->plans.clear();
   for (auto& kv : ctx->datasets) cudaFree(kv.second->block);
   ctx->datasets.clear();
   cudaFree(ctx->d_counter);
@@ -576,6 +812,11 @@ int epik2_unload(epik2_ctx* ctx, int32_t dataset_id) {
   if (it == ctx->datasets.end()) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  for (auto pit = ctx->plans.begin(); pit != ctx->plans.end();) {
+    const std::vector<int32_t>& k = pit->first;
+    if (std::find(k.begin(), k.end() - 1, dataset_id) != k.end() - 1) pit = ctx->plans.erase(pit);
+    else ++pit;
+  }
   cudaFree(it->second->block);
   ctx->datasets.erase(it);
   return EPIK2_OK;
@@ -643,6 +884,46 @@ int epik2_scan_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int
   r = epik2_scan(ctx, id, opts, out);
   epik2_unload(ctx, id);
   return r;
+}
+
+int epik2_autotune(epik2_ctx* ctx, int32_t dataset_id, epik2_tune* out) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (!out) return fail(ctx, EPIK2_E_INVALID, "null output");
+  DevDataset* d = find(ctx, dataset_id);
+  if (!d) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
+  if (d->n_snps < 3) return fail(ctx, EPIK2_E_INVALID, "need at least 3 SNPs");
+  CK(ctx, cudaSetDevice(ctx->device), "set device");
+  int r = autotune_now(ctx, *d, out);
+  if (r) return r;
+  ctx->tune_cache[shape_bucket(*d)] = *out;
+  return EPIK2_OK;
+}
+
+int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, const epik2_opts* opts, epik2_best* out) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (!dataset_ids || !out || n < 1) return fail(ctx, EPIK2_E_INVALID, "bad dataset list");
+  std::vector<DevDataset*> ds;
+  std::vector<int32_t> ids(dataset_ids, dataset_ids + n);
+  DevDataset* largest = nullptr;
+  for (int32_t b = 0; b < n; b++) {
+    DevDataset* d = find(ctx, dataset_ids[b]);
+    if (!d) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset in batch");
+    if (d->n_snps < 3) return fail(ctx, EPIK2_E_INVALID, "every dataset needs at least 3 SNPs");
+    ds.push_back(d);
+    const double w = (double)triplets_before(d->n_snps, d->n_snps) * (double)d->n_samples;
+    if (!largest || w > (double)triplets_before(largest->n_snps, largest->n_snps) * (double)largest->n_samples)
+      largest = d;
+  }
+  CK(ctx, cudaSetDevice(ctx->device), "set device");
+  int kw = (opts && opts->stage_words) ? opts->stage_words : 0;
+  if (kw != 0 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
+  if (kw == 0) {
+    epik2_tune t{};
+    int r = tuned(ctx, *largest, &t);
+    if (r) return r;
+    kw = t.stage_words;
+  }
+  return run_batch(ctx, ds, ids, kw, out);
 }
 
 int epik2_dump_tables(epik2_ctx* ctx, int32_t dataset_id, uint32_t* tables, float* scores) {

@@ -74,6 +74,19 @@ struct ScanParams {
   float* dump_scores;      // [C(m,3)] or null
 };
 
+// One dataset of a batched tensor-core search (device-resident job table).
+struct TcJob {
+  const uint2* planes;
+  const uint32_t* singles;
+  const uint4* pairs;
+  const float* lut;
+  const int64_t* pb_off;
+  const uint32_t* pb_ij;
+  int64_t n_pb;
+  int64_t tri;
+  int32_t m, m_pad, w0, w1, n0, n1;
+};
+
 // Tensor-core engine parameters (scan_tc.cu).  Tiles: for each pair block (i, j0..j0+31)
 // the k blocks [128*kb, 128*kb+128) with kb from (j0+1)/128 to ceil(m/128)-1.
 struct TcParams {
@@ -94,6 +107,11 @@ struct TcParams {
   uint32_t* dump_tables;
   float* dump_scores;
   int* err;                // set to 1 if a bounded wait expired
+  // batched form (jobs != null): tiles of job b are [job_tile_off[b], job_tile_off[b+1])
+  const TcJob* jobs;
+  const int64_t* job_tile_off;
+  int32_t n_jobs;
+  BestSlot* job_slots;     // [n_jobs][grid]
 };
 
 // Kernel launchers (scan_int.cu / scan_tc.cu / encode.cu); all asynchronous on `stream`.
@@ -105,7 +123,10 @@ cudaError_t launch_tables(const DevDataset& d, const uint32_t* triplets, int64_t
                           cudaStream_t stream);
 cudaError_t launch_rescore(const DevDataset& d, const BestSlot* cand, int64_t n, Rescored* out, cudaStream_t stream);
 int scan_blocks_per_sm();
-cudaError_t launch_scan_tc(const TcParams& p, int blocks, bool dump, cudaStream_t stream);
+cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool dump, cudaStream_t stream);
+cudaError_t launch_reduce_jobs(const BestSlot* slots, int n_jobs, int per_job, BestSlot* out, cudaStream_t stream);
+cudaError_t launch_fill_slots(BestSlot* slots, int64_t n, cudaStream_t stream);
+cudaError_t tc_configure();  // dynamic shared memory limits of the tensor-core kernels (once)
 int tc_warps_per_block();
 
 // Host helpers (host_data.cpp).

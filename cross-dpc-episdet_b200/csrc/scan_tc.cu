@@ -34,11 +34,8 @@ namespace epik2 {
 constexpr int kTcThreads = 512;  // 16 warps
 constexpr int kTcWarps = kTcThreads / 32;
 constexpr int kTcK = 128;        // SNPs k per tile  -> 256 rows of B
-constexpr int kTcStages = 4;
-constexpr int kStageA = 128 * 128;  // bytes: 128 rows x 128 samples
-constexpr int kStageB = 256 * 128;  // bytes: 256 rows x 128 samples
-constexpr int kStageBytes = kStageA + kStageB;
-constexpr int kTcSmemBytes = kTcStages * kStageBytes + 256;
+constexpr int kRingBytes = 16 * 384 * 32;  // stage ring: kStages x 384 rows x (32 * kW) bytes = 192 KiB
+constexpr int kTcSmemBytes = kRingBytes + 256;  // + mbarriers
 constexpr int kEStride = 129;  // words per row of the epilogue staging buffer
 constexpr long long kWaitLimit = 4000000000LL;  // SM clocks (~2 s) before a wait gives up
 // instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = 256, M = 128
@@ -49,9 +46,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
 }
 
 // Shared-memory matrix descriptor, no swizzle, K-major: LBO = 128 B (next 16-byte K
-// group), SBO = 1024 B (next group of 8 rows), descriptor version 1.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+// group), SBO = bytes between groups of 8 rows, descriptor version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) |
          ((uint64_t)1 << 46);
 }
 
@@ -134,20 +131,42 @@ __device__ __forceinline__ void sts128(uint32_t saddr, uint4 v) {
                : "memory");
 }
 
-template <bool kDump, bool kTopK>
+// One dataset's view for a tile: the plain search has one, the batched search reads the
+// tile's dataset from the job table.
+struct JobView {
+  const uint2* planes;
+  const uint32_t* singles;
+  const uint4* pairs;
+  const float* lut;
+  const int64_t* pb_off;
+  const uint32_t* pb_ij;
+  int64_t n_pb, tri;
+  int32_t m, m_pad, w0, w1, n0, n1;
+};
+
+// kW = class words (32 samples each) per pipeline stage: 4 (4 stages of 48 KiB) or 8 (2
+// stages of 96 KiB).  kBatched: tiles of many datasets on one queue, per-dataset results.
+template <int kW, bool kBatched, bool kDump, bool kTopK>
 __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
+  constexpr int kStages = 16 / kW;
+  constexpr int kStageA = 128 * 32 * kW;            // bytes: 128 rows x 32*kW samples
+  constexpr int kStageBytes = 384 * 32 * kW;        // A + B (256 rows)
+  constexpr uint32_t kSbo = 256 * kW;               // bytes between 8-row groups
+  constexpr int kU = kW / 4;                        // units of each kind per thread per stage
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t s_tmem;
   __shared__ long long s_tile;
   __shared__ int s_abort;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kTcStages * kStageBytes);  // [stages] empty + acc
+  __shared__ float s_red_s[kTcWarps];
+  __shared__ unsigned long long s_red_k[kTcWarps];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kRingBytes);  // [stages] empty + acc
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t stage0 = smem_u32(smem);
   const uint32_t bar0 = smem_u32(bars);
-  const uint32_t bar_acc = bar0 + 8 * kTcStages;
+  const uint32_t bar_acc = bar0 + 8 * kStages;
 
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; s++) bar_init(bar0 + 8 * s, 1);
+    for (int s = 0; s < kStages; s++) bar_init(bar0 + 8 * s, 1);
     bar_init(bar_acc, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
@@ -163,10 +182,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
   tc_fence_after();
   const uint32_t tmem = s_tmem;
 
-  const int64_t m_pad = p.m_pad;
-  const int m = p.m;
-  const int64_t tri = p.tri;
-  const int nc0 = (p.w0 + 3) >> 2, nc1 = (p.w1 + 3) >> 2, nct = nc0 + nc1;
   float best_s = FLT_MAX;
   unsigned long long best_k = ~0ull;
   float list_s = FLT_MAX;
@@ -177,74 +192,106 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
   for (;;) {
     if (tid == 0) s_tile = (long long)atomicAdd(p.counter, 1ull);
     __syncthreads();
-    const long long tile = s_tile;
+    long long tile = s_tile;
     if (tile >= p.n_tiles || s_abort) break;
-    int64_t lo = 0, hi = p.n_pb;
+    JobView jv;
+    int job = 0;
+    if (kBatched) {
+      int lo = 0, hi = p.n_jobs;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (p.job_tile_off[mid] <= tile) lo = mid;
+        else hi = mid;
+      }
+      job = lo;
+      tile -= p.job_tile_off[job];
+      const TcJob& J = p.jobs[job];
+      jv = JobView{J.planes, J.singles, J.pairs, J.lut, J.pb_off, J.pb_ij, J.n_pb, J.tri,
+                   J.m, J.m_pad, J.w0, J.w1, J.n0, J.n1};
+    } else {
+      jv = JobView{p.planes, p.singles, p.pairs, p.lut, p.pb_off, p.pb_ij, p.n_pb, p.tri,
+                   p.m, p.m_pad, p.w0, p.w1, p.n0, p.n1};
+    }
+    const int64_t m_pad = jv.m_pad;
+    const int m = jv.m;
+    const int nc0 = (jv.w0 + kW - 1) / kW, nc1 = (jv.w1 + kW - 1) / kW, nct = nc0 + nc1;
+    int64_t lo = 0, hi = jv.n_pb;
     while (hi - lo > 1) {
       const int64_t mid = (lo + hi) >> 1;
-      if (p.pb_off[mid] <= tile) lo = mid;
+      if (jv.pb_off[mid] <= tile) lo = mid;
       else hi = mid;
     }
-    const int i = (int)p.pb_ij[2 * lo], j0 = (int)p.pb_ij[2 * lo + 1];
-    const int k0 = kTcK * ((j0 + 1) / kTcK + (int)(tile - p.pb_off[lo]));
+    const int i = (int)jv.pb_ij[2 * lo], j0 = (int)jv.pb_ij[2 * lo + 1];
+    const int k0 = kTcK * ((j0 + 1) / kTcK + (int)(tile - jv.pb_off[lo]));
 
-    // ---- producer / MMA pipeline over the class words, 128 samples per stage ----
-    // Thread roles in a stage (4 class words = 128 samples):
-    //   A row r = 32*ab + q (pair q, g_i = ab>>1, g_j = ab&1), word w: ab = tid>>7,
-    //     w = (tid>>5)&3, q = lane -> one warp writes 32 consecutive rows;
-    //   B row n = 128*c + kl (k = k0+kl, g_k = c), word w: kl = tid&127, w = tid>>7.
+    // ---- operand expansion and MMA, 32*kW samples per stage ----
+    // Units of a stage, kU of each kind per thread (r < kU):
+    //   A: word w = (tid>>7) + 4r, row = tid&127 = 32*ab + q (pair q, g_i = ab>>1, g_j = ab&1)
+    //   B: word w = (tid>>7) + 4r, kl = tid&127 -> rows 128*c + kl (g_k = c) of both c
+    // A warp writes 32 consecutive rows of one 16-byte K group per store (conflict-free).
     // The words of stage cc+1 are loaded while stage cc is expanded.
-    const int a_ab = tid >> 7, a_w = (tid >> 5) & 3, a_q = lane;
-    const int a_row = 32 * a_ab + a_q;
-    const int a_j = min(j0 + a_q, (int)m_pad - 1);
-    const int b_kl = tid & 127, b_w = tid >> 7;
+    const int a_row = tid & 127, a_ab = a_row >> 5, w_base = tid >> 7;
+    const int a_j = min(j0 + (a_row & 31), (int)m_pad - 1);
+    const int b_kl = tid & 127;
     const int b_k = k0 + b_kl;
-    auto load_words = [&](int cc, uint2& gi, uint2& gj, uint2& gk) {
-      const int cls = cc < nc0 ? 0 : 1;
-      const int c_in = cls ? cc - nc0 : cc;
-      const int64_t wcls = cls ? p.w1 : p.w0;
-      const int64_t wbase = (cls ? p.w0 : 0) + 4 * c_in;
-      gi = make_uint2(0, 0);
-      gj = make_uint2(0, 0);
-      gk = make_uint2(0, 0);
-      if (4 * c_in + a_w < wcls) {
-        const uint2* row = p.planes + (wbase + a_w) * m_pad;
-        gi = __ldg(row + i);
-        gj = __ldg(row + a_j);
+    const uint32_t offa0 = (a_row >> 3) * kSbo + (a_row & 7) * 16;
+    const uint32_t offb0 = (b_kl >> 3) * kSbo + (b_kl & 7) * 16;  // + 128*kSbo/8 for c = 1
+    auto load_words = [&](int cc, uint2 (&gi)[kU], uint2 (&gj)[kU], uint2 (&gk)[kU]) {
+      const bool c1 = cc >= nc0;
+      const int c_in = c1 ? cc - nc0 : cc;
+      const int wcls = c1 ? jv.w1 : jv.w0;
+      const int64_t wb = (c1 ? (int64_t)jv.w0 : 0) + (int64_t)kW * c_in;
+#pragma unroll
+      for (int r = 0; r < kU; r++) {
+        const int w = w_base + 4 * r;
+        gi[r] = make_uint2(0, 0);
+        gj[r] = gi[r];
+        gk[r] = gi[r];
+        if (kW * c_in + w < wcls) {
+          const uint2* row = jv.planes + (wb + w) * m_pad;
+          gi[r] = __ldg(row + i);
+          gj[r] = __ldg(row + a_j);
+          if (b_k < m_pad) gk[r] = __ldg(row + b_k);
+        }
       }
-      if (4 * c_in + b_w < wcls && b_k < m_pad) gk = __ldg(p.planes + (wbase + b_w) * m_pad + b_k);
     };
-    uint2 ci, cj, ck;
+    uint2 ci[kU], cj[kU], ck[kU];
     if (nct > 0) load_words(0, ci, cj, ck);
     bool aborted = false;
     for (int cc = 0; cc < nct; ++cc, ++g_chunk) {
-      uint2 ni = make_uint2(0, 0), nj = ni, nk = ni;
+      uint2 ni[kU], nj[kU], nk[kU];
+#pragma unroll
+      for (int r = 0; r < kU; r++) ni[r] = nj[r] = nk[r] = make_uint2(0, 0);
       if (cc + 1 < nct) load_words(cc + 1, ni, nj, nk);
-      const int s = (int)(g_chunk % kTcStages);
-      const uint32_t use = g_chunk / kTcStages;
+      const int s = (int)(g_chunk % kStages);
+      const uint32_t use = g_chunk / kStages;
       bool ok = true;
       if (use > 0) ok = bar_wait(bar0 + 8 * s, (use & 1u) ^ 1u);
       if (!ok) s_abort = 1;
-      const int cls = cc < nc0 ? 0 : 1;
-      const int c_in = cls ? cc - nc0 : cc;
+      const bool c1 = cc >= nc0;
+      const int c_in = c1 ? cc - nc0 : cc;
       const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
       if (ok) {
-        const uint32_t wa = ((a_ab >> 1) ? ci.y : ci.x) & ((a_ab & 1) ? cj.y : cj.x);
-        const uint32_t offa = sA + (a_row >> 3) * 1024 + (a_row & 7) * 16 + (2 * a_w) * 128;
-        sts128(offa, expand16(wa));
-        sts128(offa + 128, expand16(wa >> 16));
 #pragma unroll
-        for (int c = 0; c < 2; c++) {
-          const int n = 128 * c + b_kl;
-          const uint32_t wb = c ? ck.y : ck.x;
-          const uint32_t offb = sB + (n >> 3) * 1024 + (n & 7) * 16 + (2 * b_w) * 128;
-          sts128(offb, expand16(wb));
-          sts128(offb + 128, expand16(wb >> 16));
+        for (int r = 0; r < kU; r++) {
+          const int w = w_base + 4 * r;
+          const uint32_t wa = ((a_ab >> 1) ? ci[r].y : ci[r].x) & ((a_ab & 1) ? cj[r].y : cj[r].x);
+          const uint32_t offa = sA + offa0 + (2 * w) * 128;
+          sts128(offa, expand16(wa));
+          sts128(offa + 128, expand16(wa >> 16));
+          const uint32_t offb = sB + offb0 + (2 * w) * 128;
+          sts128(offb, expand16(ck[r].x));
+          sts128(offb + 128, expand16(ck[r].x >> 16));
+          sts128(offb + 16 * kSbo, expand16(ck[r].y));
+          sts128(offb + 16 * kSbo + 128, expand16(ck[r].y >> 16));
         }
       }
-      ci = ni;
-      cj = nj;
-      ck = nk;
+#pragma unroll
+      for (int r = 0; r < kU; r++) {
+        ci[r] = ni[r];
+        cj[r] = nj[r];
+        ck[r] = nk[r];
+      }
       fence_proxy_async();
       __syncthreads();
       if (s_abort) {
@@ -253,10 +300,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
       }
       if (tid == 0) {
         tc_fence_after();
-        const uint32_t d = tmem + (uint32_t)(cls * 256);
+        const uint32_t d = tmem + (c1 ? 256u : 0u);
 #pragma unroll
-        for (int kk = 0; kk < 4; kk++)
-          mma_i8(d, smem_desc(sA + kk * 256), smem_desc(sB + kk * 256), (c_in > 0 || kk > 0) ? 1u : 0u);
+        for (int kk = 0; kk < kW; kk++)
+          mma_i8(d, smem_desc(sA + kk * 256, kSbo), smem_desc(sB + kk * 256, kSbo), (c_in > 0 || kk > 0) ? 1u : 0u);
         mma_commit(bar0 + 8 * s);
         if (cc == nct - 1) mma_commit(bar_acc);
       }
@@ -278,8 +325,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
     const int quarter = warp & 3, cgrp = warp >> 2;
     const int row = 32 * quarter + lane;
     const int e_c = cgrp >> 1, e_sub = cgrp & 1;
-    const uint2 si0 = *reinterpret_cast<const uint2*>(p.singles + ((int64_t)i) * 2);
-    const uint2 si1 = *reinterpret_cast<const uint2*>(p.singles + (m_pad + i) * 2);
+    const int64_t tri = jv.tri;
+    const uint2 si0 = *reinterpret_cast<const uint2*>(jv.singles + ((int64_t)i) * 2);
+    const uint2 si1 = *reinterpret_cast<const uint2*>(jv.singles + (m_pad + i) * 2);
     for (int h = 0; h < 2; h++) {
       uint32_t* Ew = reinterpret_cast<uint32_t*>(smem);
 #pragma unroll
@@ -322,18 +370,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
               t80[2 * ab + c] = E[(0 * 128 + 32 * ab + q) * kEStride + 64 * c + kl];
               t81[2 * ab + c] = E[(1 * 128 + 32 * ab + q) * kEStride + 64 * c + kl];
             }
-          const uint2 sj0 = *reinterpret_cast<const uint2*>(p.singles + ((int64_t)j) * 2);
-          const uint2 sj1 = *reinterpret_cast<const uint2*>(p.singles + (m_pad + j) * 2);
-          const uint2 sk0 = *reinterpret_cast<const uint2*>(p.singles + ((int64_t)k) * 2);
-          const uint2 sk1 = *reinterpret_cast<const uint2*>(p.singles + (m_pad + k) * 2);
+          const uint2 sj0 = *reinterpret_cast<const uint2*>(jv.singles + ((int64_t)j) * 2);
+          const uint2 sj1 = *reinterpret_cast<const uint2*>(jv.singles + (m_pad + j) * 2);
+          const uint2 sk0 = *reinterpret_cast<const uint2*>(jv.singles + ((int64_t)k) * 2);
+          const uint2 sk1 = *reinterpret_cast<const uint2*>(jv.singles + (m_pad + k) * 2);
           const int64_t oij = tri_offset(m_pad, i, j), oik = tri_offset(m_pad, i, k), ojk = tri_offset(m_pad, j, k);
-          const uint4 pij0 = __ldg(p.pairs + oij), pij1 = __ldg(p.pairs + tri + oij);
-          const uint4 pik0 = __ldg(p.pairs + oik), pik1 = __ldg(p.pairs + tri + oik);
-          const uint4 pjk0 = __ldg(p.pairs + ojk), pjk1 = __ldg(p.pairs + tri + ojk);
+          const uint4 pij0 = __ldg(jv.pairs + oij), pij1 = __ldg(jv.pairs + tri + oij);
+          const uint4 pik0 = __ldg(jv.pairs + oik), pik1 = __ldg(jv.pairs + tri + oik);
+          const uint4 pjk0 = __ldg(jv.pairs + ojk), pjk1 = __ldg(jv.pairs + tri + ojk);
           uint32_t T0[27], T1[27];
-          complete_table(t80, (uint32_t)p.n0, si0, sj0, sk0, pij0, pik0, pjk0, T0);
-          complete_table(t81, (uint32_t)p.n1, si1, sj1, sk1, pij1, pik1, pjk1, T1);
-          sc = k2_score(T0, T1, p.lut);
+          complete_table(t80, (uint32_t)jv.n0, si0, sj0, sk0, pij0, pik0, pjk0, T0);
+          complete_table(t81, (uint32_t)jv.n1, si1, sj1, sk1, pij1, pik1, pjk1, T1);
+          sc = k2_score(T0, T1, jv.lut);
           key = pack_key((uint64_t)i, (uint64_t)j, (uint64_t)k);
           if (kDump) {
             const int64_t t = triplet_index(m, i, j, k);
@@ -358,14 +406,47 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
             const int src = __ffs(want) - 1;
             want &= want - 1;
             const float cs = __shfl_sync(kFull, sc, src);
-            const unsigned long long ck = __shfl_sync(kFull, key, src);
+            const unsigned long long ck2 = __shfl_sync(kFull, key, src);
             const float ts2 = __shfl_sync(kFull, list_s, 31);
             const unsigned long long tk2 = __shfl_sync(kFull, list_k, 31);
-            if (better(cs, ck, ts2, tk2)) warp_list_insert(list_s, list_k, cs, ck, lane);
+            if (better(cs, ck2, ts2, tk2)) warp_list_insert(list_s, list_k, cs, ck2, lane);
           }
         }
       }
       __syncthreads();  // the staging buffer is rewritten by the next half / next tile
+    }
+    if (kBatched) {
+      // fold the tile's candidates into this CTA's slot of the tile's dataset
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const float os = __shfl_xor_sync(kFull, best_s, off);
+        const unsigned long long ok = __shfl_xor_sync(kFull, best_k, off);
+        if (better(os, ok, best_s, best_k)) {
+          best_s = os;
+          best_k = ok;
+        }
+      }
+      if (lane == 0) {
+        s_red_s[warp] = best_s;
+        s_red_k[warp] = best_k;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        float bs = s_red_s[0];
+        unsigned long long bk = s_red_k[0];
+        for (int w = 1; w < kTcWarps; w++)
+          if (better(s_red_s[w], s_red_k[w], bs, bk)) {
+            bs = s_red_s[w];
+            bk = s_red_k[w];
+          }
+        BestSlot& slot = p.job_slots[(int64_t)job * gridDim.x + blockIdx.x];
+        if (better(bs, bk, slot.score, slot.key)) {
+          slot.score = bs;
+          slot.key = bk;
+        }
+      }
+      best_s = FLT_MAX;
+      best_k = ~0ull;
     }
   }
 
@@ -377,44 +458,135 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
   }
+  if (!kBatched) {
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const float os = __shfl_xor_sync(kFull, best_s, off);
-    const unsigned long long ok = __shfl_xor_sync(kFull, best_k, off);
-    if (better(os, ok, best_s, best_k)) {
-      best_s = os;
-      best_k = ok;
+    for (int off = 16; off > 0; off >>= 1) {
+      const float os = __shfl_xor_sync(kFull, best_s, off);
+      const unsigned long long ok = __shfl_xor_sync(kFull, best_k, off);
+      if (better(os, ok, best_s, best_k)) {
+        best_s = os;
+        best_k = ok;
+      }
+    }
+    const int64_t gwarp = (int64_t)blockIdx.x * kTcWarps + warp;
+    if (lane == 0) {
+      p.slots[gwarp].score = best_s;
+      p.slots[gwarp].key = best_k;
+    }
+    if (kTopK) {
+      p.cand[gwarp * 32 + lane].score = list_s;
+      p.cand[gwarp * 32 + lane].key = list_k;
     }
   }
-  const int64_t gwarp = (int64_t)blockIdx.x * kTcWarps + warp;
-  if (lane == 0) {
-    p.slots[gwarp].score = best_s;
-    p.slots[gwarp].key = best_k;
+}
+
+// Per-dataset reduction of the batched search's per-CTA slots: block b reduces dataset b.
+__global__ void k_reduce_jobs(const BestSlot* __restrict__ slots, int per_job, BestSlot* __restrict__ out) {
+  __shared__ float ss[32];
+  __shared__ unsigned long long sk[32];
+  const BestSlot* js = slots + (int64_t)blockIdx.x * per_job;
+  float bs = FLT_MAX;
+  unsigned long long bk = ~0ull;
+  for (int t = threadIdx.x; t < per_job; t += blockDim.x)
+    if (better(js[t].score, js[t].key, bs, bk)) {
+      bs = js[t].score;
+      bk = js[t].key;
+    }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const float os = __shfl_xor_sync(kFull, bs, off);
+    const unsigned long long ok = __shfl_xor_sync(kFull, bk, off);
+    if (better(os, ok, bs, bk)) {
+      bs = os;
+      bk = ok;
+    }
   }
-  if (kTopK) {
-    p.cand[gwarp * 32 + lane].score = list_s;
-    p.cand[gwarp * 32 + lane].key = list_k;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    ss[w] = bs;
+    sk[w] = bk;
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    bs = lane < nw ? ss[lane] : FLT_MAX;
+    bk = lane < nw ? sk[lane] : ~0ull;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const float os = __shfl_xor_sync(kFull, bs, off);
+      const unsigned long long ok = __shfl_xor_sync(kFull, bk, off);
+      if (better(os, ok, bs, bk)) {
+        bs = os;
+        bk = ok;
+      }
+    }
+    if (lane == 0) {
+      out[blockIdx.x].score = bs;
+      out[blockIdx.x].key = bk;
+    }
+  }
+}
+
+__global__ void k_fill_slots(BestSlot* __restrict__ slots, int64_t n) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) {
+    slots[t].score = FLT_MAX;
+    slots[t].key = ~0ull;
   }
 }
 
 int tc_warps_per_block() { return kTcWarps; }
 
-cudaError_t launch_scan_tc(const TcParams& p, int blocks, bool dump, cudaStream_t stream) {
+template <int kW, bool kB, bool kD, bool kT>
+static cudaError_t set_smem() {
+  return cudaFuncSetAttribute(k_scan_tc<kW, kB, kD, kT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
+}
+
+cudaError_t tc_configure() {
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_scan_tc<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kTcSmemBytes);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_scan_tc<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_scan_tc<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
+    cudaError_t e = set_smem<4, false, false, false>();
+    if (e == cudaSuccess) e = set_smem<4, false, true, false>();
+    if (e == cudaSuccess) e = set_smem<4, false, false, true>();
+    if (e == cudaSuccess) e = set_smem<8, false, false, false>();
+    if (e == cudaSuccess) e = set_smem<8, false, true, false>();
+    if (e == cudaSuccess) e = set_smem<8, false, false, true>();
+    if (e == cudaSuccess) e = set_smem<4, true, false, false>();
+    if (e == cudaSuccess) e = set_smem<8, true, false, false>();
     if (e != cudaSuccess) return e;
     configured = true;
   }
+  return cudaSuccess;
+}
+
+cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool dump, cudaStream_t stream) {
+  const cudaError_t ce = tc_configure();
+  if (ce != cudaSuccess) return ce;
   const bool topk = p.top_k > 1;
-  if (dump) k_scan_tc<true, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
-  else if (topk) k_scan_tc<false, true><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
-  else k_scan_tc<false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+  const bool batched = p.jobs != nullptr;
+  if (words_per_stage == 8) {
+    if (batched) k_scan_tc<8, true, false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+    else if (dump) k_scan_tc<8, false, true, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+    else if (topk) k_scan_tc<8, false, false, true><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+    else k_scan_tc<8, false, false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+  } else {
+    if (batched) k_scan_tc<4, true, false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+    else if (dump) k_scan_tc<4, false, true, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+    else if (topk) k_scan_tc<4, false, false, true><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+    else k_scan_tc<4, false, false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_jobs(const BestSlot* slots, int n_jobs, int per_job, BestSlot* out, cudaStream_t stream) {
+  if (n_jobs <= 0) return cudaSuccess;
+  k_reduce_jobs<<<n_jobs, 256, 0, stream>>>(slots, per_job, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_slots(BestSlot* slots, int64_t n, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  k_fill_slots<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(slots, n);
   return cudaGetLastError();
 }
 

@@ -61,9 +61,17 @@ class Stats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class Tune(ctypes.Structure):
+    _fields_ = [("engine", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("rate_int", ctypes.c_double),
+                ("rate_tc4", ctypes.c_double), ("rate_tc8", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class Opts(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("top_k", ctypes.c_int32), ("rescore_fp64", ctypes.c_int32),
-                ("k_strip", ctypes.c_int32), ("pairs_per_warp", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("k_strip", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
                 ("snp_begin", ctypes.c_int64), ("snp_end", ctypes.c_int64)]
 
 
@@ -119,6 +127,8 @@ def library():
         "epik2_reset_stats": ([p], ctypes.c_int),
         "epik2_scan_u8_noalloc": ([p, p, i64, i64, p, ctypes.POINTER(Best)], ctypes.c_int),
         "epik2_set_engine": ([p, ctypes.c_int], ctypes.c_int),
+        "epik2_scan_batch": ([p, p, i32, ctypes.POINTER(Opts), ctypes.POINTER(Best)], ctypes.c_int),
+        "epik2_autotune": ([p, i32, ctypes.POINTER(Tune)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -316,6 +326,19 @@ class Context:
         self._check(self._lib.epik2_scan_u8(self._h, _ptr(geno), _ptr(pheno), geno.shape[0], geno.shape[1],
                                             ctypes.byref(o), ctypes.byref(b)))
         return b
+
+    def scan_batch(self, datasets, **opts):
+        """Best triplet of each dataset from one batched, graph-captured launch."""
+        ids = np.ascontiguousarray(np.asarray(datasets, dtype=np.int32))
+        o = self._opts(**opts)
+        arr = (Best * len(ids))()
+        self._check(self._lib.epik2_scan_batch(self._h, _ptr(ids), len(ids), ctypes.byref(o), arr))
+        return [arr[t] for t in range(len(ids))]
+
+    def autotune(self, dataset):
+        t = Tune()
+        self._check(self._lib.epik2_autotune(self._h, dataset, ctypes.byref(t)))
+        return t.as_dict()
 
     def dump_tables(self, dataset):
         m = self.info(dataset)["n_snps"]

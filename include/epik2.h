@@ -73,7 +73,7 @@ typedef struct {
   int32_t top_k;       /* 0/1 = best only; >1 = keep the top_k lowest FP32 scores */
   int32_t rescore_fp64;/* 1 = rescore the kept candidates in FP64 on the GPU */
   int32_t k_strip;     /* tuning: SNPs per k-strip (multiple of 32); 0 = autotuned */
-  int32_t pairs_per_warp; /* tuning: reserved, 0 = default */
+  int32_t stage_words;  /* tuning, tensor cores: 32-sample words per pipeline stage, 4 or 8; 0 = autotuned */
   int32_t blocks_per_sm;  /* tuning: 0 = occupancy-derived */
   int64_t snp_begin;   /* restrict the first index i to [snp_begin, snp_end); 0,0 = all */
   int64_t snp_end;
@@ -159,6 +159,32 @@ int epik2_scan_topk(epik2_ctx *ctx, int32_t dataset_id, const epik2_opts *opts, 
 /* One call from host buffers to the best triplet: load + scan + unload. */
 int epik2_scan_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int64_t n_samples,
                   int64_t n_snps, const epik2_opts *opts, epik2_best *out);
+
+/* --------------------------------------------------------------------------------
+ * Batched form (no reference counterpart).  One persistent tensor-core launch over many
+ * resident datasets: the triplet tiles of all of them go on one shared queue, each CTA
+ * folds its candidates into per-dataset slots, and a per-dataset reduction writes
+ * out[0..n).  The launch sequence is captured once per set of datasets into a CUDA
+ * graph and replayed (phenotype re-encodings via epik2_set_pheno are picked up).  The
+ * stage depth is opts->stage_words or, when 0, the autotuner's choice for the largest
+ * dataset.  Each result equals epik2_scan on that dataset alone.
+ * ------------------------------------------------------------------------------ */
+int epik2_scan_batch(epik2_ctx *ctx, const int32_t *dataset_ids, int32_t n, const epik2_opts *opts,
+                     epik2_best *out);
+
+/* Autotuner (no reference counterpart).  Times the integer engine and the tensor-core
+ * engine at 4 and 8 words per stage on a slice of the dataset (about 1/64 of its
+ * triplets, at least a few tiles per SM) and caches the fastest per shape bucket
+ * (log2 of samples and SNPs); EPIK2_ENGINE_AUTO scans use the cached choice.  Reports the
+ * choice and the measured rates (triplet*samples/s) of the three candidates. */
+typedef struct {
+  int32_t engine;        /* EPIK2_ENGINE_INT or EPIK2_ENGINE_TC */
+  int32_t stage_words;   /* tensor-core stage depth chosen (4 or 8) */
+  double rate_int;       /* measured rates on the slice */
+  double rate_tc4;
+  double rate_tc8;
+} epik2_tune;
+int epik2_autotune(epik2_ctx *ctx, int32_t dataset_id, epik2_tune *out);
 
 /* --------------------------------------------------------------------------------
  * Parity / inspection.  The reference keeps tables in registers (GPU/v4.cpp:317);

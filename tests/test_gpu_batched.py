@@ -1,0 +1,75 @@
+"""Batched form: one persistent, graph-captured tensor-core launch over many datasets
+(GPU).  Each dataset's result must equal a separate plain run's (and the oracle's)."""
+import numpy as np
+import pytest
+
+import epik2
+import oracle as O
+from conftest import f32_bits
+from epik2 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+MIXED = [  # (seed, samples, SNPs, cases): uneven sizes, class splits and tile counts
+    (71, 300, 20, 140), (72, 1000, 45, 333), (73, 64, 3, 32), (74, 2047, 70, 1500), (75, 500, 130, 250),
+    (76, 40, 12, 5), (77, 3001, 33, 1500), (78, 129, 257, 64), (79, 777, 64, 400), (80, 1500, 100, 600),
+]
+
+
+@pytest.mark.parametrize("stage_words", [4, 8])
+def test_batch_equals_separate_runs_and_oracle(stage_words):
+    data = [O.gen_hwe(sd, S, M, c) for sd, S, M, c in MIXED]
+    with epik2.Context(0) as ctx:
+        ids = [ctx.load(g, p) for g, p in data]
+        batched = ctx.scan_batch(ids, stage_words=stage_words)
+        again = ctx.scan_batch(ids, stage_words=stage_words)  # graph replay
+        single = [ctx.scan(d, engine=epik2.ENGINE_TC, stage_words=stage_words) for d in ids]
+        single_int = [ctx.scan(d, engine=epik2.ENGINE_INT) for d in ids]
+    for (g, p), b, b2, s, si in zip(data, batched, again, single, single_int):
+        ref = O.scan(g, p) if g.shape[1] <= 140 else None
+        assert b.ijk == s.ijk == si.ijk == b2.ijk
+        assert f32_bits(b.score) == f32_bits(s.score) == f32_bits(si.score) == f32_bits(b2.score)
+        if ref is not None:
+            assert b.ijk == ref["ijk"] and f32_bits(b.score) == f32_bits(ref["score"])
+
+
+def test_batch_follows_phenotype_reencoding():
+    g, p = O.gen_hwe(81, 900, 60, 400)
+    g2, p2 = O.gen_hwe(82, 600, 80, 300)
+    with epik2.Context(0) as ctx:
+        a, b = ctx.load(g, p), ctx.load(g2, p2)
+        first = ctx.scan_batch([a, b])
+        q = np.random.default_rng(3).permutation(p)
+        ctx.set_pheno(a, q)
+        second = ctx.scan_batch([a, b])  # same plan, new class split of dataset a
+    assert second[1].ijk == first[1].ijk
+    r = O.scan(g, q)
+    assert second[0].ijk == r["ijk"] and f32_bits(second[0].score) == f32_bits(r["score"])
+
+
+@pytest.mark.slow
+def test_batched_workload_96_datasets_equals_one_by_one():
+    specs = W.batched_specs()
+    with epik2.Context(0) as ctx:
+        ids = []
+        for sp in specs:
+            g, p = W.generate(sp)
+            ids.append(ctx.load(g, p))
+        batched = ctx.scan_batch(ids)
+        one_by_one = [ctx.scan(d) for d in ids]
+    for sp, b, s in zip(specs, batched, one_by_one):
+        assert b.ijk == s.ijk, sp["name"]
+        assert f32_bits(b.score) == f32_bits(s.score), sp["name"]
+
+
+def test_autotune_reports_all_candidates():
+    g, p = O.gen_hwe(83, 2000, 300, 1000)
+    with epik2.Context(0) as ctx:
+        d = ctx.load(g, p)
+        t = ctx.autotune(d)
+        b = ctx.scan(d)  # AUTO engine uses the cached choice
+    assert t["engine"] in (epik2.ENGINE_INT, epik2.ENGINE_TC)
+    assert t["stage_words"] in (4, 8)
+    assert min(t["rate_int"], t["rate_tc4"], t["rate_tc8"]) > 0
+    r = O.scan(g, p)
+    assert b.ijk == r["ijk"]
