@@ -61,9 +61,13 @@ struct BatchPlan {
   epik2::BestSlot* d_job_slots = nullptr;
   epik2::BestSlot* d_results = nullptr;
   epik2::BestSlot* h_results = nullptr;  // pinned
+  epik2::Rescored* d_resc = nullptr;     // FP64 rescore of each dataset's best
+  epik2::Rescored* h_resc = nullptr;     // pinned
   int* h_err = nullptr;                  // pinned
   std::vector<epik2::TcJob> h_jobs;
-  std::vector<int64_t> pb_base;          // offset of each job's pair-block list
+  std::vector<int64_t> pb_base;          // offset of each job's pair-block tile prefix sums
+  std::vector<int64_t> pb_ij_base;       // offset of each job's (i, j0) list
+  bool rescore = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   ~BatchPlan() {
@@ -77,6 +81,8 @@ struct BatchPlan {
     cudaFree(d_results);
     cudaFreeHost(h_results);
     cudaFreeHost(h_err);
+    cudaFree(d_resc);
+    cudaFreeHost(h_resc);
   }
 };
 
@@ -105,13 +111,13 @@ struct Layout {
   size_t geno, perm, planes, singles, pairs, lut, lut64, total;
 };
 
-Layout dataset_layout(int64_t s, int64_t m) {
+Layout dataset_layout(int64_t s, int64_t m, bool with_geno = true) {
   const int64_t m_pad = (m + 31) / 32 * 32;
   const int64_t words = (s + 31) / 32 + 1;  // enough for any class split
   Layout L{};
   size_t off = 0;
   L.geno = off;
-  off = align_up(off + (size_t)(s * m), 256);
+  off = align_up(off + (with_geno ? (size_t)(s * m) : 0), 256);
   L.perm = off;
   off = align_up(off + (size_t)s * 4, 256);
   L.planes = off;
@@ -471,9 +477,9 @@ int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
 // Batched form: build (or reuse) the plan for these datasets, refresh the job table from
 // the datasets' current class split, replay the captured launch sequence.
 int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vector<int32_t>& ids, int kw,
-              epik2_best* out) {
+              bool rescore, epik2_best* out) {
   std::vector<int32_t> key = ids;
-  key.push_back(kw);
+  key.push_back(kw * 2 + (rescore ? 1 : 0));
   BatchPlan* plan = nullptr;
   auto it = ctx->plans.find(key);
   const int32_t n = (int32_t)ds.size();
@@ -484,25 +490,35 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     std::unique_ptr<BatchPlan> pl(new BatchPlan());
     pl->kw = kw;
     pl->n_jobs = n;
+    pl->rescore = rescore;
+    // pair-block lists depend on the SNP count only: one list per distinct count
     std::vector<int64_t> job_off(1, 0), pb_off_all;
     std::vector<uint32_t> pb_ij_all;
+    struct ListInfo {
+      int64_t off_base, ij_base, n_pb, tiles;
+    };
+    std::map<int64_t, ListInfo> lists;
     for (int32_t b = 0; b < n; b++) {
       const int64_t m = ds[b]->n_snps, n_kb = (m + 127) / 128;
-      pl->pb_base.push_back((int64_t)pb_off_all.size());
-      int64_t tiles = 0;
-      pb_off_all.push_back(0);
-      int64_t n_pb = 0;
-      for (int64_t i = 0; i < m; i++)
-        for (int64_t j0 = i + 1; j0 <= m - 2; j0 += 32) {
-          pb_ij_all.push_back((uint32_t)i);
-          pb_ij_all.push_back((uint32_t)j0);
-          tiles += n_kb - (j0 + 1) / 128;
-          pb_off_all.push_back(tiles);
-          n_pb++;
-        }
-      job_off.push_back(job_off.back() + tiles);
+      auto li = lists.find(m);
+      if (li == lists.end()) {
+        ListInfo L{(int64_t)pb_off_all.size(), (int64_t)pb_ij_all.size(), 0, 0};
+        pb_off_all.push_back(0);
+        for (int64_t i = 0; i < m; i++)
+          for (int64_t j0 = i + 1; j0 <= m - 2; j0 += 32) {
+            pb_ij_all.push_back((uint32_t)i);
+            pb_ij_all.push_back((uint32_t)j0);
+            L.tiles += n_kb - (j0 + 1) / 128;
+            pb_off_all.push_back(L.tiles);
+            L.n_pb++;
+          }
+        li = lists.emplace(m, L).first;
+      }
+      pl->pb_base.push_back(li->second.off_base);
+      pl->pb_ij_base.push_back(li->second.ij_base);
+      job_off.push_back(job_off.back() + li->second.tiles);
       TcJob j{};
-      j.n_pb = std::max<int64_t>(n_pb, 1);
+      j.n_pb = std::max<int64_t>(li->second.n_pb, 1);
       pl->h_jobs.push_back(j);
     }
     pl->n_tiles = job_off.back();
@@ -511,7 +527,8 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
         cudaMalloc(&pl->d_pb_off, 8 * pb_off_all.size()) || cudaMalloc(&pl->d_pb_ij, pb_ij_bytes) ||
         cudaMalloc(&pl->d_job_slots, sizeof(BestSlot) * (size_t)n * grid) ||
         cudaMalloc(&pl->d_results, sizeof(BestSlot) * n) || cudaMallocHost(&pl->h_results, sizeof(BestSlot) * n) ||
-        cudaMallocHost(&pl->h_err, sizeof(int)))
+        cudaMallocHost(&pl->h_err, sizeof(int)) || cudaMalloc(&pl->d_resc, sizeof(Rescored) * n) ||
+        cudaMallocHost(&pl->h_resc, sizeof(Rescored) * n))
       return fail(ctx, EPIK2_E_NOMEM, "batched plan: device memory");
     CK(ctx, cudaMemcpyAsync(pl->d_job_off, job_off.data(), 8 * (n + 1), cudaMemcpyHostToDevice, ctx->stream),
        "upload batch");
@@ -543,6 +560,9 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream);
     if (e == cudaSuccess) e = launch_scan_tc(p, grid, kw, false, ctx->stream);
     if (e == cudaSuccess) e = launch_reduce_jobs(pl->d_job_slots, n, grid, pl->d_results, ctx->stream);
+    if (e == cudaSuccess && rescore) e = launch_rescore_jobs(pl->d_jobs, pl->d_results, n, pl->d_resc, ctx->stream);
+    if (e == cudaSuccess && rescore)
+      e = cudaMemcpyAsync(pl->h_resc, pl->d_resc, sizeof(Rescored) * n, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(pl->h_results, pl->d_results, sizeof(BestSlot) * n, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(pl->h_err, ctx->d_err, 4, cudaMemcpyDeviceToHost, ctx->stream);
@@ -562,7 +582,8 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     j.pairs = d.pairs;
     j.lut = d.lut;
     j.pb_off = plan->d_pb_off + plan->pb_base[b];
-    j.pb_ij = plan->d_pb_ij + 2 * (plan->pb_base[b] - b);
+    j.pb_ij = plan->d_pb_ij + plan->pb_ij_base[b];
+    j.lut64 = d.lut64;
     j.tri = d.tri;
     j.m = (int32_t)d.n_snps;
     j.m_pad = (int32_t)d.m_pad;
@@ -591,7 +612,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
   for (int32_t b = 0; b < n; b++) {
     const BestSlot& r = plan->h_results[b];
     out[b].score = r.score;
-    out[b].score_fp64 = std::numeric_limits<double>::quiet_NaN();
+    out[b].score_fp64 = rescore ? plan->h_resc[b].s64 : std::numeric_limits<double>::quiet_NaN();
     decode_key(r.key, out[b].i, out[b].j, out[b].k);
   }
   return EPIK2_OK;
@@ -806,15 +827,75 @@ int epik2_set_pheno(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* pheno) {
   return encode_with(ctx, *d, pheno);
 }
 
+int64_t epik2_replicate_bytes(int64_t n_samples, int64_t n_snps) {
+  if (n_samples < 1 || n_snps < 1) return -1;
+  return (int64_t)dataset_layout(n_samples, n_snps, false).total;
+}
+
+int epik2_load_replicate(epik2_ctx* ctx, int32_t base_dataset_id, const uint8_t* pheno, int32_t* dataset_id) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (!pheno || !dataset_id) return fail(ctx, EPIK2_E_INVALID, "null pointer");
+  DevDataset* base = find(ctx, base_dataset_id);
+  if (!base) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
+  int32_t root_id = base->base_id >= 0 ? base->base_id : base_dataset_id;
+  DevDataset* root = find(ctx, root_id);
+  if (!root) return fail(ctx, EPIK2_E_NOT_FOUND, "genotype owner no longer loaded");
+  CK(ctx, cudaSetDevice(ctx->device), "set device");
+  const Layout L = dataset_layout(root->n_samples, root->n_snps, false);
+  size_t fr = 0, tot = 0;
+  CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
+  if (L.total + (size_t)(256u << 20) > fr) return fail(ctx, EPIK2_E_NOMEM, "replicate does not fit in free device memory");
+  std::unique_ptr<DevDataset> d(new DevDataset());
+  CK(ctx, cudaMalloc(&d->block, L.total), "alloc replicate");
+  char* b = (char*)d->block;
+  d->bytes = L.total;
+  d->n_samples = root->n_samples;
+  d->n_snps = root->n_snps;
+  d->m_pad = root->m_pad;
+  d->tri = root->tri;
+  d->geno = root->geno;
+  d->perm = (int32_t*)(b + L.perm);
+  d->planes = (uint2*)(b + L.planes);
+  d->singles = (uint32_t*)(b + L.singles);
+  d->pairs = (uint4*)(b + L.pairs);
+  d->lut = (float*)(b + L.lut);
+  d->lut64 = (double*)(b + L.lut64);
+  d->base_id = root_id;
+  cudaError_t e = cudaMemcpyAsync(d->lut, root->lut, (size_t)(root->n_samples + 2) * 4, cudaMemcpyDeviceToDevice,
+                                  ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d->lut64, root->lut64, (size_t)(root->n_samples + 2) * 8, cudaMemcpyDeviceToDevice,
+                        ctx->stream);
+  if (e != cudaSuccess) {
+    cudaFree(d->block);
+    return cuda_fail(ctx, e, "replicate tables");
+  }
+  int r = encode_with(ctx, *d, pheno);
+  if (r) {
+    cudaFree(d->block);
+    return r;
+  }
+  root->n_replicates++;
+  const int32_t id = ctx->next_id++;
+  ctx->datasets[id] = std::move(d);
+  *dataset_id = id;
+  return EPIK2_OK;
+}
+
 int epik2_unload(epik2_ctx* ctx, int32_t dataset_id) {
   if (!ctx) return EPIK2_E_INVALID;
   auto it = ctx->datasets.find(dataset_id);
   if (it == ctx->datasets.end()) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
+  if (it->second->n_replicates > 0) return fail(ctx, EPIK2_E_BUSY, "dataset still has live replicates");
+  if (it->second->base_id >= 0) {
+    DevDataset* root = find(ctx, it->second->base_id);
+    if (root) root->n_replicates--;
+  }
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   for (auto pit = ctx->plans.begin(); pit != ctx->plans.end();) {
     const std::vector<int32_t>& k = pit->first;
-    if (std::find(k.begin(), k.end() - 1, dataset_id) != k.end() - 1) pit = ctx->plans.erase(pit);
+    if (std::find(k.begin(), k.end() - 1, dataset_id) != k.end() - 1) pit = ctx->plans.erase(pit);  // last: variant
     else ++pit;
   }
   cudaFree(it->second->block);
@@ -923,7 +1004,7 @@ int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, cons
     if (r) return r;
     kw = t.stage_words;
   }
-  return run_batch(ctx, ds, ids, kw, out);
+  return run_batch(ctx, ds, ids, kw, opts && opts->rescore_fp64, out);
 }
 
 int epik2_dump_tables(epik2_ctx* ctx, int32_t dataset_id, uint32_t* tables, float* scores) {

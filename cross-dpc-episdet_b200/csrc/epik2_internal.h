@@ -28,6 +28,8 @@ struct DevDataset {
   int64_t tri = 0;              // entries per class in `pairs`
   void* block = nullptr;        // single allocation holding all of the above
   size_t bytes = 0;
+  int32_t base_id = -1;         // replicate: dataset whose genotype matrix this one shares
+  int32_t n_replicates = 0;     // live replicates sharing this dataset's genotypes
 };
 
 // Offset of pair (x, y), x < y, in a row-major strict upper triangle of an m x m matrix.
@@ -80,6 +82,7 @@ struct TcJob {
   const uint32_t* singles;
   const uint4* pairs;
   const float* lut;
+  const double* lut64;
   const int64_t* pb_off;
   const uint32_t* pb_ij;
   int64_t n_pb;
@@ -126,7 +129,8 @@ int scan_blocks_per_sm();
 cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool dump, cudaStream_t stream);
 cudaError_t launch_reduce_jobs(const BestSlot* slots, int n_jobs, int per_job, BestSlot* out, cudaStream_t stream);
 cudaError_t launch_fill_slots(BestSlot* slots, int64_t n, cudaStream_t stream);
-cudaError_t tc_configure();  // dynamic shared memory limits of the tensor-core kernels (once)
+cudaError_t tc_configure();
+cudaError_t launch_rescore_jobs(const TcJob* jobs, const BestSlot* best, int n, Rescored* out, cudaStream_t stream);  // dynamic shared memory limits of the tensor-core kernels (once)
 int tc_warps_per_block();
 
 // Host helpers (host_data.cpp).

@@ -328,6 +328,47 @@ cudaError_t launch_reduce_best(const BestSlot* slots, int n, BestSlot* out, cuda
   return cudaGetLastError();
 }
 
+// FP64 rescore of each batched dataset's best triplet (one warp per dataset).
+__global__ void k_rescore_jobs(const TcJob* __restrict__ jobs, const BestSlot* __restrict__ best, int n,
+                               Rescored* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int b = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (b >= n) return;
+  const unsigned long long key = best[b].key;
+  if (key == ~0ull) {
+    if (lane == 0) {
+      out[b].s64 = 0.0;
+      out[b].s32 = FLT_MAX;
+      out[b].key = key;
+    }
+    return;
+  }
+  const TcJob& J = jobs[b];
+  const int64_t i = (int64_t)(key >> 42), j = (int64_t)((key >> 21) & 0x1fffff), k = (int64_t)(key & 0x1fffff);
+  uint32_t cnt[54];
+  warp_direct_table(J.planes, J.m_pad, J.w0, J.w1, J.n0, J.n1, i, j, k, lane, cnt);
+  if (lane == 0) {
+    float s32 = 0.0f;
+    double s64 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 27; c++) {
+      const uint32_t x = cnt[c], y = cnt[27 + c];
+      s32 = __fadd_rn(s32, __fsub_rn(__fsub_rn(J.lut[x + y + 1], J.lut[x]), J.lut[y]));
+      s64 = __dadd_rn(s64, __dsub_rn(__dsub_rn(J.lut64[x + y + 1], J.lut64[x]), J.lut64[y]));
+    }
+    out[b].s64 = fabs(s64);
+    out[b].s32 = fabsf(s32);
+    out[b].key = key;
+  }
+}
+
+cudaError_t launch_rescore_jobs(const TcJob* jobs, const BestSlot* best, int n, Rescored* out, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t threads = (int64_t)n * 32;
+  k_rescore_jobs<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(jobs, best, n, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_rescore(const DevDataset& d, const BestSlot* cand, int64_t n, Rescored* out,
                            cudaStream_t stream) {
   if (n == 0) return cudaSuccess;

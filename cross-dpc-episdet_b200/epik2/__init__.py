@@ -69,6 +69,21 @@ class Tune(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_reserve_bytes", ctypes.c_int64), ("batch_work", ctypes.c_double), ("max_active", ctypes.c_int32),
+                ("max_queued", ctypes.c_int32), ("rescore_fp64", ctypes.c_int32), ("stage_words", ctypes.c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("rejected", ctypes.c_int64),
+                ("cancelled", ctypes.c_int64), ("scans_queued", ctypes.c_int64), ("scans_active", ctypes.c_int64),
+                ("scans_done", ctypes.c_int64), ("launches", ctypes.c_int64), ("triplet_samples", ctypes.c_double),
+                ("busy_seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class Opts(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("top_k", ctypes.c_int32), ("rescore_fp64", ctypes.c_int32),
                 ("k_strip", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
@@ -129,6 +144,17 @@ def library():
         "epik2_set_engine": ([p, ctypes.c_int], ctypes.c_int),
         "epik2_scan_batch": ([p, p, i32, ctypes.POINTER(Opts), ctypes.POINTER(Best)], ctypes.c_int),
         "epik2_autotune": ([p, i32, ctypes.POINTER(Tune)], ctypes.c_int),
+        "epik2_load_replicate": ([p, i32, p, ctypes.POINTER(i32)], ctypes.c_int),
+        "epik2_replicate_bytes": ([i64, i64], i64),
+        "epik2_server_create": ([ctypes.POINTER(p), ctypes.c_int, ctypes.POINTER(ServerOpts)], ctypes.c_int),
+        "epik2_server_destroy": ([p], None),
+        "epik2_server_add_matrix": ([p, p, p, i64, i64, ctypes.POINTER(i32)], ctypes.c_int),
+        "epik2_server_submit_replicates": ([p, i32, p, i32, ctypes.POINTER(i64)], ctypes.c_int),
+        "epik2_server_submit_scan": ([p, p, p, i64, i64, ctypes.POINTER(i64)], ctypes.c_int),
+        "epik2_server_poll": ([p, i64, ctypes.POINTER(Best), i32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)],
+                              ctypes.c_int),
+        "epik2_server_cancel": ([p, i64], ctypes.c_int),
+        "epik2_server_get_stats": ([p, ctypes.POINTER(ServerStats)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -340,6 +366,12 @@ class Context:
         self._check(self._lib.epik2_autotune(self._h, dataset, ctypes.byref(t)))
         return t.as_dict()
 
+    def load_replicate(self, dataset, pheno):
+        pheno = np.ascontiguousarray(pheno, dtype=np.uint8)
+        did = ctypes.c_int32()
+        self._check(self._lib.epik2_load_replicate(self._h, dataset, _ptr(pheno), ctypes.byref(did)))
+        return did.value
+
     def dump_tables(self, dataset):
         m = self.info(dataset)["n_snps"]
         T = n_triplets(m)
@@ -368,3 +400,97 @@ def probe_int_peaks(device=0):
     if r:
         raise Epik2Error(r, "probe failed")
     return {"popc_per_s": a.value, "lop3_per_s": b.value, "iadd_per_s": c.value}
+
+
+class Server:
+    """Continuous-batching request server (epik2_server_*): one device context, one
+    worker thread, requests from any thread."""
+
+    def __init__(self, device=0, **opts):
+        self._lib = library()
+        o = ServerOpts()
+        for k, v in opts.items():
+            setattr(o, k, v)
+        h = ctypes.c_void_p()
+        r = self._lib.epik2_server_create(ctypes.byref(h), device, ctypes.byref(o))
+        if r:
+            raise Epik2Error(r, strerror(r))
+        self._h = h
+        self._sizes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.epik2_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_matrix(self, geno, pheno):
+        geno = np.ascontiguousarray(geno, dtype=np.uint8)
+        pheno = np.ascontiguousarray(pheno, dtype=np.uint8)
+        mid = ctypes.c_int32()
+        r = self._lib.epik2_server_add_matrix(self._h, _ptr(geno), _ptr(pheno), geno.shape[0], geno.shape[1],
+                                              ctypes.byref(mid))
+        if r:
+            raise Epik2Error(r, strerror(r))
+        self._sizes[mid.value] = geno.shape[0]
+        return mid.value
+
+    def submit_replicates(self, matrix, phenos):
+        phenos = np.ascontiguousarray(phenos, dtype=np.uint8)
+        rid = ctypes.c_int64()
+        r = self._lib.epik2_server_submit_replicates(self._h, matrix, _ptr(phenos), phenos.shape[0], ctypes.byref(rid))
+        if r:
+            raise Epik2Error(r, strerror(r))
+        return rid.value
+
+    def submit_scan(self, geno, pheno):
+        geno = np.ascontiguousarray(geno, dtype=np.uint8)
+        pheno = np.ascontiguousarray(pheno, dtype=np.uint8)
+        rid = ctypes.c_int64()
+        r = self._lib.epik2_server_submit_scan(self._h, _ptr(geno), _ptr(pheno), geno.shape[0], geno.shape[1],
+                                               ctypes.byref(rid))
+        if r:
+            raise Epik2Error(r, strerror(r))
+        return rid.value
+
+    def poll(self, request, capacity=1024):
+        """None while running; (status, [Best], latency_s) once done (record released)."""
+        arr = (Best * capacity)()
+        n = ctypes.c_int32()
+        lat = ctypes.c_double()
+        r = self._lib.epik2_server_poll(self._h, request, arr, capacity, ctypes.byref(n), ctypes.byref(lat))
+        if r == E_BUSY:
+            return None
+        if r == E_NOT_FOUND:
+            raise Epik2Error(r, "unknown request")
+        return r, [arr[t] for t in range(n.value)], lat.value
+
+    def wait(self, request, timeout=600.0, capacity=1024):
+        import time
+        t0 = time.time()
+        while True:
+            res = self.poll(request, capacity)
+            if res is not None:
+                return res
+            if time.time() - t0 > timeout:
+                raise TimeoutError(f"request {request} not done after {timeout} s")
+            time.sleep(0.002)
+
+    def cancel(self, request):
+        return self._lib.epik2_server_cancel(self._h, request)
+
+    def stats(self):
+        st = ServerStats()
+        self._lib.epik2_server_get_stats(self._h, ctypes.byref(st))
+        return st.as_dict()

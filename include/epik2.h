@@ -139,6 +139,14 @@ int epik2_load_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int
                   int64_t n_snps, int32_t *dataset_id);
 /* Re-encode a resident dataset with a new phenotype vector (permutation replicate). */
 int epik2_set_pheno(epik2_ctx *ctx, int32_t dataset_id, const uint8_t *pheno);
+/* A new dataset that shares the genotype matrix of a resident dataset (no upload) and
+ * has its own phenotype: the unit of a permutation-replicate scan (no reference
+ * counterpart).  The genotype owner cannot be unloaded while replicates of it live
+ * (EPIK2_E_BUSY). */
+int epik2_load_replicate(epik2_ctx *ctx, int32_t base_dataset_id, const uint8_t *pheno, int32_t *dataset_id);
+/* Device bytes a replicate of this shape holds (its planes and margins, not the shared
+ * genotypes). */
+int64_t epik2_replicate_bytes(int64_t n_samples, int64_t n_snps);
 int epik2_unload(epik2_ctx *ctx, int32_t dataset_id);
 /* n_samples, n_snps, n_cases, and device bytes held by the dataset. */
 int epik2_dataset_info(const epik2_ctx *ctx, int32_t dataset_id, int64_t *n_samples, int64_t *n_snps,
@@ -185,6 +193,51 @@ typedef struct {
   double rate_tc8;
 } epik2_tune;
 int epik2_autotune(epik2_ctx *ctx, int32_t dataset_id, epik2_tune *out);
+
+/* --------------------------------------------------------------------------------
+ * Serving form (no reference counterpart).  A request server owns a device context and
+ * one worker thread.  Requests arrive at any time from any thread: either a set of
+ * phenotype-permutation replicates against a genotype matrix kept resident in HBM, or a
+ * fresh genotype matrix with its phenotype.  The worker batches continuously: before each
+ * batched launch it admits queued replicate scans (oldest first) while free device memory
+ * (above a reserve), a work target per launch and a slot limit allow, so scans of
+ * different requests run in the same launch; memory and slots freed by a launch admit the
+ * next scans.  A request completes when all its scans have; its latency is completion
+ * time minus submission time.
+ * ------------------------------------------------------------------------------ */
+typedef struct epik2_server epik2_server;
+typedef struct {
+  int64_t hbm_reserve_bytes; /* device memory left unused by admission; 0 = 2 GiB */
+  double batch_work;         /* triplet*samples to aim for per launch; 0 = 2e13 */
+  int32_t max_active;        /* scans per launch at most; 0 = 256 */
+  int32_t max_queued;        /* queued scans beyond which submissions are refused; 0 = 1 << 20 */
+  int32_t rescore_fp64;      /* 1 = FP64 rescore of every scan's best triplet */
+  int32_t stage_words;       /* tensor-core stage depth, 0 = autotuned */
+} epik2_server_opts;
+typedef struct {
+  int64_t submitted, completed, rejected, cancelled; /* requests */
+  int64_t scans_queued, scans_active, scans_done;    /* single scans (replicates) */
+  int64_t launches;
+  double triplet_samples; /* completed work */
+  double busy_seconds;    /* worker time inside batched launches */
+} epik2_server_stats;
+int epik2_server_create(epik2_server **out, int device, const epik2_server_opts *opts);
+void epik2_server_destroy(epik2_server *srv);
+/* Keep a genotype matrix (with a reference phenotype) resident for replicate requests. */
+int epik2_server_add_matrix(epik2_server *srv, const uint8_t *geno, const uint8_t *pheno, int64_t n_samples,
+                            int64_t n_snps, int32_t *matrix_id);
+/* phenos: n_replicates x n_samples bytes, one phenotype per replicate. */
+int epik2_server_submit_replicates(epik2_server *srv, int32_t matrix_id, const uint8_t *phenos,
+                                   int32_t n_replicates, int64_t *request_id);
+int epik2_server_submit_scan(epik2_server *srv, const uint8_t *geno, const uint8_t *pheno, int64_t n_samples,
+                             int64_t n_snps, int64_t *request_id);
+/* EPIK2_E_BUSY while the request runs; EPIK2_OK once done: out[r] = best triplet of scan r
+ * (r < min(capacity, scans)), *latency_seconds set, and the request record released.
+ * A refused or failed request reports its status here. */
+int epik2_server_poll(epik2_server *srv, int64_t request_id, epik2_best *out, int32_t capacity, int32_t *n_out,
+                      double *latency_seconds);
+int epik2_server_cancel(epik2_server *srv, int64_t request_id);
+int epik2_server_get_stats(epik2_server *srv, epik2_server_stats *out);
 
 /* --------------------------------------------------------------------------------
  * Parity / inspection.  The reference keeps tables in registers (GPU/v4.cpp:317);
