@@ -45,26 +45,6 @@ def env_int(name, default):
         return default
 
 
-def shard_bounds(m, parts):
-    """Cut first indices [0, m) into `parts` contiguous ranges of near-equal triplet count."""
-    work = [((m - 1 - i) * (m - 2 - i)) // 2 for i in range(m)]
-    total = sum(work)
-    bounds, acc, lo = [], 0, 0
-    for i in range(m):
-        acc += work[i]
-        if len(bounds) < parts - 1 and acc >= total * (len(bounds) + 1) / parts:
-            bounds.append((lo, i + 1))
-            lo = i + 1
-    bounds.append((lo, m))
-    while len(bounds) < parts:
-        bounds.append((m, m))
-    return bounds
-
-
-def triplets_in(m, lo, hi):
-    return sum(((m - 1 - i) * (m - 2 - i)) // 2 for i in range(lo, hi))
-
-
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
@@ -187,6 +167,7 @@ def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
     import epik2
+    from epik2 import sharding as SH
     from epik2 import workloads as W
 
     torch.cuda.set_device(local_rank)
@@ -209,12 +190,20 @@ def run_ours(args, rank, world, local_rank):
     info = ctx.info(did)
     words = (info["n_samples"] - info["n_cases"] + 31) // 32 + (info["n_cases"] + 31) // 32
     parts = max(args.shards, world)
-    shards = shard_bounds(M, parts)
+    shards = SH.shard_bounds(M, parts)
     peaks = epik2.probe_int_peaks(local_rank)
+    tune = ctx.autotune(did)  # AUTO-engine scans below use this choice
+    engine_tc = tune["engine"] == epik2.ENGINE_TC
     flush = torch.empty(args.flush_mb << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
 
     def shard_of(t):
         return shards[(t * world + rank) % parts]
+
+    def exchange(b):
+        # the one exchange step of the sharded search: lowest (score, index) over ranks
+        if dist is None:
+            return b.score, b.ijk
+        return SH.exchange_best(b.score, b.ijk)
 
     def step(t):
         lo, hi = shard_of(t)
@@ -244,7 +233,7 @@ def run_ours(args, rank, world, local_rank):
         st = ctx.stats()
         kernel_ms.append(st["last_scan_kernel_ms"])
         step_trip.append(st["last_scan_triplets"])
-        bests.append((b.score, b.ijk))
+        bests.append(exchange(b))
     ev1.record(ext)
     torch.cuda.synchronize()
     barrier()
@@ -265,17 +254,36 @@ def run_ours(args, rank, world, local_rank):
         elapsed_max, ts_total = elapsed_ms, ts_local
     value = ts_total / (elapsed_max / 1e3)
 
-    # roofline of the search kernel: algorithmic popcounts (8 per triplet per 32-sample
-    # class word) over the kernel's own event-timed duration, against the measured POPC rate
-    achieved_popc = popc_local / (sum(kernel_ms) / 1e3)
+    # roofline of the search kernel over its own event-timed duration.  Tensor-core engine:
+    # algorithmic int8 ops = 2 x 8 multiply-accumulates (the 8 counted cells) per triplet
+    # per sample, against the measured dense int8 tcgen05 rate.  Integer engine: 8 POPC per
+    # triplet per 32-sample class word, against the measured POPC rate.
+    kernel_s = sum(kernel_ms) / 1e3
+    achieved_popc = popc_local / kernel_s
+    ref_form_popc = sum(step_trip) * words * 27 / kernel_s
+    kernel_name = "k_scan_tc" if engine_tc else "k_scan_int"
     traffic = None
     try:
-        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["k_scan_int"]
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))[kernel_name]
         if tr["workload"] == cfg["name"]:
             traffic = tr["dram_bytes_per_triplet"] * sum(step_trip) / len(step_trip)
     except (OSError, KeyError, ValueError):
         pass
-    ref_form_popc = sum(step_trip) * words * 27 / (sum(kernel_ms) / 1e3)
+    if engine_tc and "tc_i8_mac_per_s" in peaks:
+        ops = 16.0 * ts_local / kernel_s
+        roof = {"bound": "tensor", "achieved": ops / 1e12, "peak": 2 * peaks["tc_i8_mac_per_s"] / 1e12,
+                "unit": "TOPS (int8)", "frac": ops / (2 * peaks["tc_i8_mac_per_s"]),
+                "peak_source": "measured live by epik2_probe_tc_i8 on this GPU (dense tcgen05 kind::i8)",
+                "algorithmic_ops_per_triplet_sample": 16}
+    else:
+        roof = {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": peaks["popc_per_s"] / 1e9,
+                "unit": "Gpopc/s", "frac": achieved_popc / peaks["popc_per_s"],
+                "peak_source": "measured live by epik2_probe_int_peaks on this GPU",
+                "algorithmic_popc_per_triplet_word": 8}
+    roof.update({"traffic": traffic, "traffic_source": "ncu dram bytes per triplet (profiles/traffic.json) x triplets "
+                 "per launch", "kernel": kernel_name, "kernel_ms_per_step": sum(kernel_ms) / len(kernel_ms),
+                 "popc_equivalent_frac": achieved_popc / peaks["popc_per_s"],
+                 "reference_form_popc_frac": ref_form_popc / peaks["popc_per_s"]})
 
     # end to end through the one-call entry point, pinned host buffers
     e2e = None
@@ -296,6 +304,7 @@ def run_ours(args, rank, world, local_rank):
             lo, hi = shard_of(t)
             b = ctx.scan_u8(gn, pn, snp_begin=lo, snp_end=hi)
             e_trip += ctx.stats()["last_scan_triplets"]
+            exchange(b)
         e1.record(ext)
         torch.cuda.synchronize()
         barrier()
@@ -332,14 +341,11 @@ def run_ours(args, rank, world, local_rank):
             "config": {"workload": cfg["name"], "form": "plain", "n_snps": M, "n_samples": S,
                        "n_cases": info["n_cases"], "step": f"1/{parts} of the triplet space (first-index shard)",
                        "l2": f"flushed before every step ({args.flush_mb} MiB write)",
-                       "parallelism": f"{world} GPU(s), shard-parallel", "engine": "integer (LOP3+POPC)"},
-            "roofline": {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": peaks["popc_per_s"] / 1e9,
-                         "unit": "Gpopc/s", "frac": achieved_popc / peaks["popc_per_s"], "traffic": traffic,
-                         "traffic_source": "ncu dram bytes per triplet (profiles/traffic.json) x triplets per launch",
-                         "peak_source": "measured live by epik2_probe_int_peaks on this GPU",
-                         "algorithmic_popc_per_triplet_word": 8,
-                         "reference_form_frac": ref_form_popc / peaks["popc_per_s"],
-                         "kernel_ms_per_step": sum(kernel_ms) / len(kernel_ms)},
+                       "parallelism": f"{world} GPU(s), shard-parallel",
+                       "engine": ("tensor cores (tcgen05 int8), %d words per stage" % tune["stage_words"]) if engine_tc
+                       else "integer (LOP3+POPC)",
+                       "autotune_rates": {"int": tune["rate_int"], "tc4": tune["rate_tc4"], "tc8": tune["rate_tc8"]}},
+            "roofline": roof,
             "clocks": clocks,
             "gpu_launches": launches,
             "e2e": e2e,
@@ -355,6 +361,205 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+def _clock_ctx():
+    import torch
+    pci = None
+    try:
+        pci = torch.cuda.get_device_properties(0).pci_bus_id
+    except Exception:
+        pass
+    return ClockSampler(pci)
+
+
+def run_batched(args):
+    """Batched workload: 96 datasets (SNPs log-uniform 128..1536, samples log-uniform
+    1000..12000, case fraction 0.3..0.7) in one graph-captured tensor-core launch, against
+    the same datasets scanned one by one (one epik2_scan each)."""
+    import numpy as np
+    import epik2
+    from epik2 import workloads as W
+    specs = W.batched_specs()
+    ctx = epik2.Context(0)
+    ids = []
+    ts_total = 0.0
+    for sp in specs:
+        g, p = W.generate(sp)
+        ids.append(ctx.load(g, p))
+        ts_total += epik2.n_triplets(sp["n_snps"]) * sp["n_samples"]
+    for _ in range(max(1, args.warmup)):
+        ctx.scan_batch(ids)
+        for d in ids:
+            ctx.scan(d)
+    sampler = _clock_ctx()
+    sampler.start()
+    batch_ms, obo_ms, obo_wall = [], [], []
+    for _ in range(args.steps):
+        best_b = ctx.scan_batch(ids)
+        batch_ms.append(ctx.stats()["last_scan_kernel_ms"])
+        t0 = time.perf_counter()
+        k_ms = 0.0
+        best_o = []
+        for d in ids:
+            best_o.append(ctx.scan(d))
+            k_ms += ctx.stats()["last_scan_kernel_ms"]
+        obo_wall.append((time.perf_counter() - t0) * 1e3)
+        obo_ms.append(k_ms)
+    clocks = sampler.stop()
+    same = all(a.ijk == b.ijk and a.score == b.score for a, b in zip(best_b, best_o))
+    v_b = ts_total / (np.median(batch_ms) / 1e3)
+    v_o = ts_total / (np.median(obo_wall) / 1e3)
+    line = {"metric": METRIC, "value": v_b, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(np.median(batch_ms)), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (96 seeded Hardy-Weinberg datasets)",
+            "config": {"workload": "batched 96 datasets", "form": "batched",
+                       "triplet_samples_per_step": ts_total, "step": "one batched launch over all 96 datasets"},
+            "one_by_one": {"value": v_o, "ms_per_step": float(np.median(obo_wall)),
+                           "kernel_ms_per_step": float(np.median(obo_ms)),
+                           "what": "96 separate epik2_scan calls, wall time (host setup, launches, syncs)"},
+            "speedup_vs_one_by_one": v_b / v_o, "results_identical": same, "clocks": clocks}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def run_precision(args):
+    """Precision workload (2048 SNPs x 8192 samples, three planted triplets): plain FP32
+    search vs search + per-warp top-32 + FP64 rescore on the GPU."""
+    import numpy as np
+    import epik2
+    from epik2 import workloads as W
+    cfg = W.PRECISION
+    g, p = W.generate(cfg)
+    ctx = epik2.Context(0)
+    did = ctx.load(g, p)
+    ts = epik2.n_triplets(cfg["n_snps"]) * cfg["n_samples"]
+    for _ in range(max(1, args.warmup)):
+        ctx.scan(did)
+        ctx.scan_topk(did, 32, rescore_fp64=1)
+    plain_ms, prec_ms = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        b = ctx.scan(did)
+        plain_ms.append((time.perf_counter() - t0) * 1e3)
+        t0 = time.perf_counter()
+        top = ctx.scan_topk(did, 32, rescore_fp64=1)
+        prec_ms.append((time.perf_counter() - t0) * 1e3)
+    err = [abs(t.score - t.score_fp64) / t.score_fp64 for t in top]
+    line = {"metric": METRIC, "value": ts / (np.median(prec_ms) / 1e3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median(prec_ms)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 counts, f32 K2, f64 rescore",
+            "data": "synthetic (seeded Hardy-Weinberg, MAF 0.01..0.5, planted triplets at 0.6/0.7/0.8)",
+            "config": {"workload": cfg["name"], "form": "precision", "top_k": 32},
+            "plain": {"value": ts / (np.median(plain_ms) / 1e3), "ms_per_step": float(np.median(plain_ms))},
+            "k2_rel_error_fp32_vs_fp64": {"max": max(err), "median": float(np.median(err))},
+            "top1": {"ijk": list(top[0].ijk), "score_fp32": top[0].score, "score_fp64": top[0].score_fp64,
+                     "same_as_plain": top[0].ijk == b.ijk},
+            "top32": [list(t.ijk) for t in top]}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def run_serving(args):
+    """Serving workload: resident matrices A (1024 SNPs x 8192 samples) and B (3072 x
+    4096); Poisson arrivals; each request 16..1000 phenotype-permutation replicates of a
+    random resident matrix, 10% a fresh 256..768-SNP x 4096-sample matrix.  Reports the
+    offered and sustained load, completed/refused requests and p50/p99 latency.  A second
+    run offers half the measured capacity with 16-replicate requests on A (latency at a
+    sustainable rate)."""
+    import numpy as np
+    import epik2
+    from epik2 import workloads as W
+    spec = W.SERVING
+    rng = np.random.default_rng(spec["seed"])
+
+    def serve(rate, duration, req_maker, drain, srv_opts):
+        srv = epik2.Server(0, **srv_opts)
+        mats = []
+        for m in spec["resident"]:
+            g, p = W.generate(m)
+            mats.append((srv.add_matrix(g, p), p, m))
+        # pool of permuted phenotypes per matrix (replicates draw consecutive pool entries)
+        pools = [np.stack([rng.permutation(p) for _ in range(256)]) for _, p, _ in mats]
+        t_start = time.perf_counter()
+        next_t = t_start
+        pending, offered, refused, work_offered = [], 0, 0, 0.0
+        while time.perf_counter() - t_start < duration:
+            now = time.perf_counter()
+            if now < next_t:
+                time.sleep(min(next_t - now, 0.01))
+                continue
+            next_t += rng.exponential(1.0 / rate)
+            offered += 1
+            kind, payload, work = req_maker(mats, pools)
+            work_offered += work
+            try:
+                rid = srv.submit_replicates(*payload) if kind == "rep" else srv.submit_scan(*payload)
+                pending.append((rid, time.perf_counter()))
+            except epik2.Epik2Error:
+                refused += 1
+        t_stop = time.perf_counter()
+        lat, done = [], 0
+        deadline = t_stop + drain
+        while pending and time.perf_counter() < deadline:
+            still = []
+            for rid, t0 in pending:
+                r = srv.poll(rid)
+                if r is None:
+                    still.append((rid, t0))
+                else:
+                    done += 1
+                    if r[0] == epik2.OK:
+                        lat.append(r[2])
+            pending = still
+            time.sleep(0.01)
+        st = srv.stats()
+        wall = time.perf_counter() - t_start
+        srv.close()
+        return {"arrival_rate_per_s": rate, "duration_s": duration, "offered_requests": offered,
+                "refused_requests": refused, "completed_requests": len(lat), "unfinished_requests": len(pending),
+                "offered_triplet_samples_per_s": work_offered / duration,
+                "sustained_triplet_samples_per_s": st["triplet_samples"] / wall,
+                "latency_s": {"p50": float(np.percentile(lat, 50)) if lat else None,
+                              "p99": float(np.percentile(lat, 99)) if lat else None},
+                "scans_done": st["scans_done"], "launches": st["launches"],
+                "busy_fraction": st["busy_seconds"] / wall}
+
+    def full_request(mats, pools):
+        if rng.random() < spec["upload_frac"]:
+            m = int(rng.integers(spec["upload_snps"][0], spec["upload_snps"][1] + 1))
+            g, p = epik2.generate_hwe(int(rng.integers(1 << 30)), 4096, m, 2048)
+            return "scan", (g, p), epik2.n_triplets(m) * 4096
+        a = int(rng.integers(len(mats)))
+        n = int(rng.integers(spec["replicates"][0], spec["replicates"][1] + 1))
+        mid, p, m = mats[a]
+        start = int(rng.integers(256))
+        ph = np.take(pools[a], np.arange(start, start + n) % 256, axis=0)
+        return "rep", (mid, ph), n * epik2.n_triplets(m["n_snps"]) * m["n_samples"]
+
+    srv_opts = dict(rescore_fp64=1, max_queued=20000)
+    full = serve(spec["rate_per_s"], args.serve_seconds, full_request, args.serve_drain, srv_opts)
+    cap = full["sustained_triplet_samples_per_s"] / max(full["busy_fraction"], 1e-9)
+    light_work = 16 * epik2.n_triplets(spec["resident"][0]["n_snps"]) * spec["resident"][0]["n_samples"]
+    light_rate = max(0.05, 0.5 * cap / light_work)
+
+    def light_request(mats, pools):
+        mid, p, m = mats[0]
+        start = int(rng.integers(256))
+        ph = np.take(pools[0], np.arange(start, start + 16) % 256, axis=0)
+        return "rep", (mid, ph), light_work
+
+    light = serve(light_rate, args.serve_seconds, light_request, args.serve_drain, srv_opts)
+    line = {"metric": "p50/p99 scan latency; triplet*samples/s", "value": light["latency_s"]["p50"], "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "steps": None, "warmup": None, "vs_baseline": None,
+            "dtype": "u32 counts, f32 K2, f64 rescore", "data": "synthetic (seeded Hardy-Weinberg)",
+            "config": {"workload": "serving: resident A 1024x8192, B 3072x4096", "form": "serving"},
+            "offered_load_as_configured": full, "half_capacity_16_replicates_on_A": light,
+            "capacity_triplet_samples_per_s": cap}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -366,10 +571,19 @@ def main():
     ap.add_argument("--flush-mb", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "precision", "serving"])
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--serve-drain", type=float, default=30.0)
     args = ap.parse_args()
     rank, world, local_rank = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.form == "batched":
+        return run_batched(args)
+    if args.form == "precision":
+        return run_precision(args)
+    if args.form == "serving":
+        return run_serving(args)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -60,6 +60,74 @@ __global__ void k_iadd(uint32_t* out, int iters, uint32_t seed) {
   out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// Back-to-back tcgen05.mma kind::i8 M128 N256 K32 from zeroed shared memory (no-swizzle
+// K-major descriptors, LBO 128 B, SBO 1024 B), 512 tensor-memory columns per CTA.
+constexpr uint32_t kIdescProbe = (2u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr int kProbeSmem = 153600;  // > half an SM's shared memory: one CTA per SM
+
+__device__ __forceinline__ uint64_t probe_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46);
+}
+
+__global__ void __launch_bounds__(128, 1) k_tc_i8(int n_mma, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ uint32_t s_tmem;
+  __shared__ __align__(8) uint64_t bar;
+  const int tid = threadIdx.x;
+  for (int t = tid; t < 49152 / 4; t += blockDim.x) reinterpret_cast<uint32_t*>(smem)[t] = 0;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+  const uint32_t sbar = (uint32_t)__cvta_generic_to_shared(&bar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sbar), "r"(1u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (tid < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(&s_tmem)),
+                 "r"(512u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  if (tid == 0) {
+    for (int q = 0; q < n_mma; q++) {
+      const int kk = q & 3;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+              tmem + ((q >> 2) & 1) * 256),
+          "l"(probe_desc(sbase + kk * 256)), "l"(probe_desc(sbase + 16384 + kk * 256)), "r"(kIdescProbe),
+          "r"(q > 1 ? 1u : 0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(sbar) : "memory");
+    uint32_t ok = 0;
+    const long long t0 = clock64();
+    while (!ok) {
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, "
+          "p;\n\t}\n"
+          : "=r"(ok)
+          : "r"(sbar), "r"(0u)
+          : "memory");
+      if (clock64() - t0 > 4000000000LL) {
+        atomicExch(err, 1);
+        break;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (tid < 32) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+  }
+}
+
 typedef void (*probe_fn)(uint32_t*, int, uint32_t);
 
 int time_probe(probe_fn f, int blocks, int threads, int iters, uint32_t* d_out, double* ops_per_s) {
@@ -98,4 +166,38 @@ extern "C" int epik2_probe_int_peaks(int device, double* popc_per_s, double* lop
   if (!r) r = time_probe(k_iadd, blocks, threads, 60000, d_out, iadd_per_s);
   cudaFree(d_out);
   return r;
+}
+
+extern "C" int epik2_probe_tc_i8(int device, double* mac_per_s) {
+  if (!mac_per_s) return -1;
+  if (cudaSetDevice(device) != cudaSuccess) return -7;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return -7;
+  int* d_err = nullptr;
+  if (cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) return -3;
+  cudaMemset(d_err, 0, sizeof(int));
+  if (cudaFuncSetAttribute(k_tc_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, kProbeSmem) != cudaSuccess) {
+    cudaFree(d_err);
+    return -2;
+  }
+  const int n_mma = 16384;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_tc_i8<<<sms, 128, kProbeSmem>>>(1024, d_err);
+  cudaEventRecord(e0);
+  k_tc_i8<<<sms, 128, kProbeSmem>>>(n_mma, d_err);
+  cudaEventRecord(e1);
+  int r = cudaEventSynchronize(e1) == cudaSuccess ? 0 : -2;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  int herr = 0;
+  cudaMemcpy(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_err);
+  if (r) return r;
+  if (herr) return -6;
+  *mac_per_s = (double)n_mma * 128.0 * 256.0 * 32.0 * sms / (ms * 1e-3);
+  return 0;
 }

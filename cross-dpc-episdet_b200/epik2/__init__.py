@@ -399,7 +399,13 @@ def probe_int_peaks(device=0):
     r = L.epik2_probe_int_peaks(device, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
     if r:
         raise Epik2Error(r, "probe failed")
-    return {"popc_per_s": a.value, "lop3_per_s": b.value, "iadd_per_s": c.value}
+    out = {"popc_per_s": a.value, "lop3_per_s": b.value, "iadd_per_s": c.value}
+    L.epik2_probe_tc_i8.argtypes = [ctypes.c_int, d]
+    L.epik2_probe_tc_i8.restype = ctypes.c_int
+    m = ctypes.c_double()
+    if L.epik2_probe_tc_i8(device, ctypes.byref(m)) == 0:
+        out["tc_i8_mac_per_s"] = m.value
+    return out
 
 
 class Server:

@@ -15,6 +15,12 @@ extern "C" {
 /* Results in instructions per second per device (thread-level operations). */
 int epik2_probe_int_peaks(int device, double *popc_per_s, double *lop3_per_s, double *iadd_per_s);
 
+/* Dense int8 tensor-core rate: one CTA per SM issues back-to-back tcgen05.mma kind::i8
+ * (M=128, N=256, K=32, shared-memory operands in the search kernel's layout, int32
+ * accumulators in tensor memory); result in multiply-accumulates per second.  Waits are
+ * bounded; returns -6 if one expired. */
+int epik2_probe_tc_i8(int device, double *mac_per_s);
+
 #ifdef __cplusplus
 }
 #endif
