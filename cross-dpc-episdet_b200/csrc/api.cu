@@ -46,9 +46,13 @@ struct epik2_ctx {
   std::vector<epik2_best> last_topk;
   // autotuner choices per (log2 samples, log2 SNPs)
   std::map<std::pair<int, int>, epik2_tune> tune_cache;
-  // batched-form plans, keyed by the dataset ids
-  std::map<std::vector<int32_t>, std::unique_ptr<struct BatchPlan>> plans;
+  // batched-form plans, keyed by the SNP count of every job (a plan holds no dataset
+  // pointer: the job table is rewritten before every replay), least recently used first
+  std::map<std::vector<int64_t>, std::unique_ptr<struct BatchPlan>> plans;
+  std::vector<std::vector<int64_t>> plan_lru;
 };
+
+constexpr size_t kMaxPlans = 32;  // cached batched plans per context
 
 struct BatchPlan {
   int kw = 4;
@@ -478,15 +482,27 @@ int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
 // the datasets' current class split, replay the captured launch sequence.
 int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vector<int32_t>& ids, int kw,
               bool rescore, epik2_best* out) {
-  std::vector<int32_t> key = ids;
+  std::vector<int64_t> key;
+  for (const DevDataset* d : ds) key.push_back(d->n_snps);
   key.push_back(kw * 2 + (rescore ? 1 : 0));
   BatchPlan* plan = nullptr;
   auto it = ctx->plans.find(key);
   const int32_t n = (int32_t)ds.size();
   const int grid = ctx->tc_blocks;
+  auto touch = [&](const std::vector<int64_t>& k) {
+    auto pos = std::find(ctx->plan_lru.begin(), ctx->plan_lru.end(), k);
+    if (pos != ctx->plan_lru.end()) ctx->plan_lru.erase(pos);
+    ctx->plan_lru.push_back(k);
+  };
   if (it != ctx->plans.end()) {
     plan = it->second.get();
+    touch(key);
   } else {
+    if (ctx->plans.size() >= kMaxPlans && !ctx->plan_lru.empty()) {  // drop the least recently used
+      CK(ctx, cudaStreamSynchronize(ctx->stream), "plan eviction");
+      ctx->plans.erase(ctx->plan_lru.front());
+      ctx->plan_lru.erase(ctx->plan_lru.begin());
+    }
     std::unique_ptr<BatchPlan> pl(new BatchPlan());
     pl->kw = kw;
     pl->n_jobs = n;
@@ -572,6 +588,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     if (e != cudaSuccess) return cuda_fail(ctx, e, "batched graph");
     plan = pl.get();
     ctx->plans[key] = std::move(pl);
+    touch(key);
   }
   // refresh the job table (class splits may have changed since the plan was built)
   for (int32_t b = 0; b < n; b++) {
@@ -893,11 +910,6 @@ int epik2_unload(epik2_ctx* ctx, int32_t dataset_id) {
   }
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  for (auto pit = ctx->plans.begin(); pit != ctx->plans.end();) {
-    const std::vector<int32_t>& k = pit->first;
-    if (std::find(k.begin(), k.end() - 1, dataset_id) != k.end() - 1) pit = ctx->plans.erase(pit);  // last: variant
-    else ++pit;
-  }
   cudaFree(it->second->block);
   ctx->datasets.erase(it);
   return EPIK2_OK;

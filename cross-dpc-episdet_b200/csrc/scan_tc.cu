@@ -13,14 +13,18 @@
 //                          = count of (g_i=a, g_j=b, g_k=c) in class C.
 // A (128 x S_C) holds the pair indicators of the 32 pairs (i, j) x (a, b), B (256 x S_C)
 // the single indicators of the 128 SNPs k x c; both are expanded from the bit planes to
-// int8 (0 or -1) by the CTA's threads, 128 samples per pipeline stage, straight into shared
-// memory in the no-swizzle K-major layout the tensor core reads (8-row x 16-byte core
-// matrices; K-neighbours 128 B apart, 8-row groups 1024 B apart).  One thread issues
-// tcgen05.mma (M=128, N=256, K=32, int32 accumulators in tensor memory): class 0 into
-// TMEM columns [0,256), class 1 into [256,512).  tcgen05.commit arrives on per-stage
-// mbarriers that release the stage to the producers, and on an accumulator barrier at
-// the end of the tile; the epilogue moves the accumulators TMEM -> registers -> shared
-// memory and completes, scores and selects the 32 x 128 triplets of the tile.
+// int8 (0 or -1), 32*kW samples per pipeline stage, straight into shared memory in the
+// no-swizzle K-major layout the tensor core reads (8-row x 16-byte core matrices;
+// K-neighbours 128 B apart).  Warp roles: 16 warps expand operands (and later run the
+// epilogue); one more warp only issues tcgen05.mma (M=128, N=256, K=32, int32 accumulators
+// in tensor memory: class 0 into TMEM columns [0,256), class 1 into [256,512)).  An MMA
+// issue blocks its thread for about the MMA's execution time, so the issuing thread does
+// nothing else.  Hand-off per stage: each producing warp fences its stores for the async
+// proxy and arrives once on the stage's "full" mbarrier; the issuer waits on it, issues
+// the stage's MMAs and commits them to the stage's "empty" mbarrier, which the producers
+// wait on before refilling the slot (and, at the end of a tile, to the accumulator
+// barrier).  The epilogue moves the accumulators TMEM -> registers -> shared memory and
+// completes, scores and selects the 32 x 128 triplets of the tile.
 //
 // Every wait on an mbarrier is bounded (about 2 s of SM clock); on expiry the kernel sets
 // an error word, stops taking tiles, frees its tensor memory and returns.
@@ -31,8 +35,9 @@
 
 namespace epik2 {
 
-constexpr int kTcThreads = 512;  // 16 warps
+constexpr int kTcThreads = 512;  // 16 operand-producing / epilogue warps
 constexpr int kTcWarps = kTcThreads / 32;
+constexpr int kTcThreadsAll = kTcThreads + 32;  // + one warp that only issues the MMAs
 constexpr int kTcK = 128;        // SNPs k per tile  -> 256 rows of B
 constexpr int kRingBytes = 16 * 384 * 32;  // stage ring: kStages x 384 rows x (32 * kW) bytes = 192 KiB
 constexpr int kTcSmemBytes = kRingBytes + 256;  // + mbarriers
@@ -62,6 +67,10 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, 
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void bar_arrive(uint32_t bar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ void bar_init(uint32_t bar, uint32_t count) {
@@ -147,7 +156,7 @@ struct JobView {
 // kW = class words (32 samples each) per pipeline stage: 4 (4 stages of 48 KiB) or 8 (2
 // stages of 96 KiB).  kBatched: tiles of many datasets on one queue, per-dataset results.
 template <int kW, bool kBatched, bool kDump, bool kTopK>
-__global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
+__global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) {
   constexpr int kStages = 16 / kW;
   constexpr int kStageA = 128 * 32 * kW;            // bytes: 128 rows x 32*kW samples
   constexpr int kStageBytes = 384 * 32 * kW;        // A + B (256 rows)
@@ -164,10 +173,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
   const uint32_t stage0 = smem_u32(smem);
   const uint32_t bar0 = smem_u32(bars);
   const uint32_t bar_acc = bar0 + 8 * kStages;
+  const uint32_t bar_full0 = bar_acc + 8;  // [stages]: one arrival per producing warp
+  volatile int* abort_flag = &s_abort;
+  const bool worker = warp < kTcWarps;
 
   if (tid == 0) {
     for (int s = 0; s < kStages; s++) bar_init(bar0 + 8 * s, 1);
     bar_init(bar_acc, 1);
+    for (int s = 0; s < kStages; s++) bar_init(bar_full0 + 8 * s, kTcWarps);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
   }
@@ -255,23 +268,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
         }
       }
     };
-    uint2 ci[kU], cj[kU], ck[kU];
-    if (nct > 0) load_words(0, ci, cj, ck);
-    bool aborted = false;
-    for (int cc = 0; cc < nct; ++cc, ++g_chunk) {
-      uint2 ni[kU], nj[kU], nk[kU];
+    if (worker) {
+      uint2 ci[kU], cj[kU], ck[kU];
+      if (nct > 0) load_words(0, ci, cj, ck);
+      for (int cc = 0; cc < nct; ++cc) {
+        const uint32_t g = g_chunk + (uint32_t)cc;
+        uint2 ni[kU], nj[kU], nk[kU];
 #pragma unroll
-      for (int r = 0; r < kU; r++) ni[r] = nj[r] = nk[r] = make_uint2(0, 0);
-      if (cc + 1 < nct) load_words(cc + 1, ni, nj, nk);
-      const int s = (int)(g_chunk % kStages);
-      const uint32_t use = g_chunk / kStages;
-      bool ok = true;
-      if (use > 0) ok = bar_wait(bar0 + 8 * s, (use & 1u) ^ 1u);
-      if (!ok) s_abort = 1;
-      const bool c1 = cc >= nc0;
-      const int c_in = c1 ? cc - nc0 : cc;
-      const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
-      if (ok) {
+        for (int r = 0; r < kU; r++) ni[r] = nj[r] = nk[r] = make_uint2(0, 0);
+        if (cc + 1 < nct) load_words(cc + 1, ni, nj, nk);
+        const int s = (int)(g % kStages);
+        const uint32_t use = g / kStages;
+        const bool late = use > 0 && !bar_wait(bar0 + 8 * s, (use & 1u) ^ 1u);
+        if (__any_sync(kFull, late)) *abort_flag = 1;
+        if (__shfl_sync(kFull, *abort_flag, 0)) break;  // warp-uniform
+        const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
 #pragma unroll
         for (int r = 0; r < kU; r++) {
           const int w = w_base + 4 * r;
@@ -285,37 +296,50 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
           sts128(offb + 16 * kSbo, expand16(ck[r].y));
           sts128(offb + 16 * kSbo + 128, expand16(ck[r].y >> 16));
         }
-      }
 #pragma unroll
-      for (int r = 0; r < kU; r++) {
-        ci[r] = ni[r];
-        cj[r] = nj[r];
-        ck[r] = nk[r];
+        for (int r = 0; r < kU; r++) {
+          ci[r] = ni[r];
+          cj[r] = nj[r];
+          ck[r] = nk[r];
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) bar_arrive(bar_full0 + 8 * s);
       }
-      fence_proxy_async();
-      __syncthreads();
-      if (s_abort) {
-        aborted = true;
-        break;
-      }
-      if (tid == 0) {
+    } else if (lane == 0) {
+      // the issuing warp: wait for each stage's operands, issue its MMAs, release it
+      for (int cc = 0; cc < nct; ++cc) {
+        const uint32_t g = g_chunk + (uint32_t)cc;
+        const int s = (int)(g % kStages);
+        const uint32_t use = g / kStages;
+        if (!bar_wait(bar_full0 + 8 * s, use & 1u)) {
+          *abort_flag = 1;
+          break;
+        }
         tc_fence_after();
+        const bool c1 = cc >= nc0;
+        const int c_in = c1 ? cc - nc0 : cc;
+        const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
         const uint32_t d = tmem + (c1 ? 256u : 0u);
+        const uint64_t da = smem_desc(sA, kSbo), db = smem_desc(sB, kSbo);
 #pragma unroll
         for (int kk = 0; kk < kW; kk++)
-          mma_i8(d, smem_desc(sA + kk * 256, kSbo), smem_desc(sB + kk * 256, kSbo), (c_in > 0 || kk > 0) ? 1u : 0u);
+          mma_i8(d, da + (uint64_t)(16 * kk), db + (uint64_t)(16 * kk), (c_in > 0 || kk > 0) ? 1u : 0u);
         mma_commit(bar0 + 8 * s);
         if (cc == nct - 1) mma_commit(bar_acc);
       }
     }
-    if (aborted) break;
+    g_chunk += (uint32_t)nct;
+    __syncwarp();
+    __syncthreads();  // every thread has left the stage loop (done, or an expired wait)
+    if (*abort_flag) break;
 
     // ---- epilogue: TMEM -> shared -> complete tables, score, select ----
     {
       const bool ok = bar_wait(bar_acc, n_tile & 1u);
-      if (!ok) s_abort = 1;
+      if (!ok) *abort_flag = 1;
       __syncthreads();
-      if (s_abort) break;
+      if (*abort_flag) break;
     }
     tc_fence_after();
     ++n_tile;
@@ -332,7 +356,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
       uint32_t* Ew = reinterpret_cast<uint32_t*>(smem);
 #pragma unroll
       for (int cls = 0; cls < 2; cls++) {
-        const bool has = cls ? nc1 > 0 : nc0 > 0;
+        const bool has = (cls ? nc1 > 0 : nc0 > 0) && worker;
 #pragma unroll
         for (int part = 0; part < 2; part++) {
           const int col = 128 * e_c + 64 * h + 32 * e_sub + 16 * part;  // inside the class accumulator
@@ -345,15 +369,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
             for (int t = 0; t < 16; t++) v[t] = 0;
           }
           uint32_t* dst = Ew + (cls * 128 + row) * kEStride + 64 * e_c + 32 * e_sub + 16 * part;
+          if (worker) {
 #pragma unroll
-          for (int t = 0; t < 16; t++) dst[t] = v[t];
+            for (int t = 0; t < 16; t++) dst[t] = v[t];
+          }
         }
       }
       tc_fence_before();
       __syncthreads();
       // 32 pairs x 64 k of this half: triplet x = tid + 512u -> kl = x & 63, q = x >> 6
 #pragma unroll 1
-      for (int u = 0; u < 4; u++) {
+      for (int u = 0; u < (worker ? 4 : 0); u++) {
         const int x = tid + kTcThreads * u;
         const int kl = x & 63, q = x >> 6;
         const int j = j0 + q;
@@ -426,7 +452,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
           best_k = ok;
         }
       }
-      if (lane == 0) {
+      if (lane == 0 && worker) {
         s_red_s[warp] = best_s;
         s_red_k[warp] = best_k;
       }
@@ -458,7 +484,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(const TcParams p) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
   }
-  if (!kBatched) {
+  if (!kBatched && worker) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       const float os = __shfl_xor_sync(kFull, best_s, off);
@@ -565,15 +591,15 @@ cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, b
   const bool topk = p.top_k > 1;
   const bool batched = p.jobs != nullptr;
   if (words_per_stage == 8) {
-    if (batched) k_scan_tc<8, true, false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
-    else if (dump) k_scan_tc<8, false, true, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
-    else if (topk) k_scan_tc<8, false, false, true><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
-    else k_scan_tc<8, false, false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+    if (batched) k_scan_tc<8, true, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+    else if (dump) k_scan_tc<8, false, true, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+    else if (topk) k_scan_tc<8, false, false, true><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+    else k_scan_tc<8, false, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
   } else {
-    if (batched) k_scan_tc<4, true, false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
-    else if (dump) k_scan_tc<4, false, true, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
-    else if (topk) k_scan_tc<4, false, false, true><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
-    else k_scan_tc<4, false, false, false><<<blocks, kTcThreads, kTcSmemBytes, stream>>>(p);
+    if (batched) k_scan_tc<4, true, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+    else if (dump) k_scan_tc<4, false, true, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+    else if (topk) k_scan_tc<4, false, false, true><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+    else k_scan_tc<4, false, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
   }
   return cudaGetLastError();
 }

@@ -1,13 +1,16 @@
 // Request server with continuous batching (include/epik2.h, "Serving form").
 //
 // Host C++ on top of the public C ABI only: one epik2 context, one worker thread.  The
-// worker repeats: admit queued scans (oldest first) while the launch's work target, its
-// slot limit and free device memory above the reserve allow; create each admitted scan's
-// dataset (a replicate sharing a resident genotype matrix, or a freshly uploaded matrix);
-// run one batched launch over all of them (epik2_scan_batch); release the datasets; and
-// complete the requests whose scans are all done.  Requests that arrive during a launch
-// wait for the next admission round.
+// worker repeats: admit queued scans while the launch's work target, its slot limit and
+// free device memory above the reserve allow, taking one scan per pending request in
+// turn (round robin from where the previous round stopped, so a small request is not held
+// behind a large one); create each admitted scan's dataset (a replicate sharing a
+// resident genotype matrix, or a freshly uploaded matrix); run one batched launch over
+// all of them (epik2_scan_batch); release the datasets; and complete the requests whose
+// scans are all done.  Requests that arrive during a launch join the next admission
+// round.  Submitting never waits for the device: it copies the request and queues it.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -31,6 +34,7 @@ struct Request {
   int32_t dataset = -1;        // resident genotype owner (replicates) or -1 (fresh matrix)
   int64_t n_samples = 0, n_snps = 0;
   int32_t n_scans = 0;
+  int32_t n_admitted = 0;       // scans handed to a launch (or finished unlaunched)
   std::vector<uint8_t> phenos;  // n_scans x n_samples
   std::vector<uint8_t> geno;    // fresh matrix only
   std::vector<epik2_best> results;
@@ -46,6 +50,11 @@ struct Item {
   int32_t scan;
 };
 
+struct Matrix {
+  int32_t dataset;
+  int64_t n_samples, n_snps;
+};
+
 double work_of(int64_t s, int64_t m) { return (double)m * (double)(m - 1) * (double)(m - 2) / 6.0 * (double)s; }
 
 }  // namespace
@@ -57,13 +66,14 @@ struct epik2_server {
   std::condition_variable cv;
   std::thread worker;
   bool stop = false;
-  std::map<int32_t, int32_t> matrices;  // matrix id -> dataset id
+  std::map<int32_t, Matrix> matrices;  // matrix id -> resident dataset
   std::map<int64_t, std::unique_ptr<Request>> requests;
-  std::deque<Item> queue;
+  std::deque<Request*> pending;  // requests with scans not yet admitted, in turn order
   int64_t next_request = 1;
   int32_t next_matrix = 1;
   epik2_server_stats stats{};
   std::mutex ctx_mu;  // the context is used by the worker and by add_matrix
+  std::atomic<int> ctx_waiters{0};  // add_matrix calls waiting for ctx_mu: the worker lets them in
 
   void finish_scan(Request* r, int32_t scan, const epik2_best* res, int status) {
     if (res) r->results[(size_t)scan] = *res;
@@ -88,7 +98,7 @@ struct epik2_server {
       std::vector<Item> batch;
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv.wait(lk, [&] { return stop || !queue.empty(); });
+        cv.wait(lk, [&] { return stop || !pending.empty(); });
         if (stop) return;
         size_t free_b = 0, total_b = 0;
         {
@@ -97,29 +107,44 @@ struct epik2_server {
         }
         int64_t budget = (int64_t)free_b - reserve;
         double work = 0.0;
-        while (!queue.empty() && (int32_t)batch.size() < max_active && work < target) {
-          Item it = queue.front();
-          Request* r = it.req;
-          if (r->cancelled) {
-            queue.pop_front();
-            stats.scans_queued--;
-            finish_scan(r, it.scan, nullptr, EPIK2_E_CANCELLED);
+        // one scan per pending request in turn; a request leaves the turn order once all
+        // its scans are admitted, and the next round starts after the last request served
+        size_t blocked = 0;  // consecutive requests whose next scan does not fit now
+        while (!pending.empty() && (int32_t)batch.size() < max_active && work < target &&
+               blocked < pending.size()) {
+          Request* r = pending.front();
+          pending.pop_front();
+          const int32_t scan = r->n_admitted;
+          if (r->cancelled) {  // finish every scan not yet launched
+            for (int32_t k = scan; k < r->n_scans; k++) {
+              stats.scans_queued--;
+              finish_scan(r, k, nullptr, EPIK2_E_CANCELLED);
+            }
+            r->n_admitted = r->n_scans;
             continue;
           }
           const int64_t bytes = r->dataset >= 0 ? epik2_replicate_bytes(r->n_samples, r->n_snps)
                                                 : epik2_dataset_bytes(r->n_samples, r->n_snps);
-          if (bytes > (int64_t)total_b - reserve) {  // can never fit: refuse the scan
-            queue.pop_front();
-            stats.scans_queued--;
-            finish_scan(r, it.scan, nullptr, EPIK2_E_NOMEM);
+          if (bytes > (int64_t)total_b - reserve) {  // can never fit: refuse the request's scans
+            for (int32_t k = scan; k < r->n_scans; k++) {
+              stats.scans_queued--;
+              finish_scan(r, k, nullptr, EPIK2_E_NOMEM);
+            }
+            r->n_admitted = r->n_scans;
             continue;
           }
-          if (bytes > budget) break;  // admitted once a launch frees memory
+          if (bytes > budget) {  // admitted once a launch frees memory
+            pending.push_back(r);
+            blocked++;
+            continue;
+          }
+          blocked = 0;
           budget -= bytes;
-          queue.pop_front();
+          r->n_admitted++;
           stats.scans_queued--;
-          batch.push_back(it);
+          batch.push_back(Item{r, scan});
           work += work_of(r->n_samples, r->n_snps);
+          if (r->n_admitted < r->n_scans) pending.push_back(r);
         }
         stats.scans_active = (int64_t)batch.size();
       }
@@ -133,6 +158,8 @@ struct epik2_server {
       std::vector<size_t> ok_items;
       std::vector<int> status(batch.size(), EPIK2_OK);
       std::vector<epik2_best> res;
+      for (int spin = 0; spin < 1000 && ctx_waiters.load() > 0; spin++)  // let add_matrix in first
+        std::this_thread::sleep_for(std::chrono::microseconds(100));
       {
         std::lock_guard<std::mutex> g(ctx_mu);
         for (size_t b = 0; b < batch.size(); b++) {
@@ -215,14 +242,16 @@ int epik2_server_add_matrix(epik2_server* srv, const uint8_t* geno, const uint8_
   if (!srv || !matrix_id) return EPIK2_E_INVALID;
   int32_t id = -1;
   int r;
+  srv->ctx_waiters++;
   {
     std::lock_guard<std::mutex> g(srv->ctx_mu);
+    srv->ctx_waiters--;
     r = epik2_load_u8(srv->ctx, geno, pheno, n_samples, n_snps, &id);
   }
   if (r != EPIK2_OK) return r;
   std::lock_guard<std::mutex> lk(srv->mu);
   const int32_t mid = srv->next_matrix++;
-  srv->matrices[mid] = id;
+  srv->matrices[mid] = Matrix{id, n_samples, n_snps};
   *matrix_id = mid;
   return EPIK2_OK;
 }
@@ -239,7 +268,7 @@ static int submit(epik2_server* srv, std::unique_ptr<Request> r, int64_t* reques
   r->t_submit = Clock::now();
   r->results.assign((size_t)r->n_scans, epik2_best{});
   Request* raw = r.get();
-  for (int32_t k = 0; k < r->n_scans; k++) srv->queue.push_back(Item{raw, k});
+  srv->pending.push_back(raw);
   srv->stats.scans_queued += r->n_scans;
   *request_id = raw->id;
   srv->requests[raw->id] = std::move(r);
@@ -255,17 +284,12 @@ int epik2_server_submit_replicates(epik2_server* srv, int32_t matrix_id, const u
     std::lock_guard<std::mutex> lk(srv->mu);
     auto it = srv->matrices.find(matrix_id);
     if (it == srv->matrices.end()) return EPIK2_E_NOT_FOUND;
-    r->dataset = it->second;
+    r->dataset = it->second.dataset;
+    r->n_samples = it->second.n_samples;
+    r->n_snps = it->second.n_snps;
   }
-  int64_t s = 0, m = 0;
-  {
-    std::lock_guard<std::mutex> g(srv->ctx_mu);
-    if (epik2_dataset_info(srv->ctx, r->dataset, &s, &m, nullptr, nullptr) != EPIK2_OK) return EPIK2_E_NOT_FOUND;
-  }
-  r->n_samples = s;
-  r->n_snps = m;
   r->n_scans = n_replicates;
-  r->phenos.assign(phenos, phenos + (size_t)n_replicates * (size_t)s);
+  r->phenos.assign(phenos, phenos + (size_t)n_replicates * (size_t)r->n_samples);
   return submit(srv, std::move(r), request_id);
 }
 
