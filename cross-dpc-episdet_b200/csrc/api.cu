@@ -26,7 +26,7 @@ struct epik2_ctx {
   std::map<int32_t, std::unique_ptr<DevDataset>> datasets;
   int32_t next_id = 1;
   // search scratch
-  int engine = 0;               // default engine: 0 = auto (tensor cores), 1 = integer, 2 = tensor cores
+  int engine = 0;               // default engine: 0 = auto, 1 = integer, 2 = tensor cores int8, 3 = tensor cores FP4
   int scan_blocks = 0;          // integer engine grid
   int tc_blocks = 0;            // tensor-core engine grid (one CTA per SM)
   int n_slots = 0;              // per-warp slots, enough for either grid
@@ -202,7 +202,10 @@ int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
 
 int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_k, int n_warps);
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
-                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw);
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4);
+
+// FP4 accumulators are FP32: counts are exact below 2^24 per class.
+bool fp4_exact(const DevDataset& d) { return d.n_controls < (1 << 24) && d.n_cases < (1 << 24); }
 int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out);
 int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* dump_tables, float* dump_scores,
              BestSlot* best_out);
@@ -222,21 +225,35 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
     }
     if (opts->top_k < 0 || opts->top_k > 32) return fail(ctx, EPIK2_E_INVALID, "top_k must be in [0, 32]");
     top_k = opts->top_k;
-    if (opts->engine < 0 || opts->engine > 2) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
+    if (opts->engine < 0 || opts->engine > EPIK2_ENGINE_TC_FP4) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
   }
   if (ie < ib) ie = ib;
   int engine = ctx->engine;
   if (opts && opts->engine != 0) engine = opts->engine;
   int kw = (opts && opts->stage_words) ? opts->stage_words : 0;
-  if (kw != 0 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
-  if (engine == 0 || (engine == 2 && kw == 0)) {
+  if (engine == EPIK2_ENGINE_TC_FP4 && !fp4_exact(d))
+    return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
+  if (engine == 0 || ((engine == 2 || engine == 3) && kw == 0)) {
     epik2_tune t{};
     int r = tuned(ctx, d, &t);
     if (r) return r;
-    if (engine == 0) engine = t.engine;
-    if (kw == 0) kw = t.stage_words;
+    if (engine == 0) {  // a requested stage depth that only one format takes picks that format
+      engine = t.engine;
+      if (kw == 4 && engine == 3) engine = 2;
+      if (kw == 16 && engine == 2 && fp4_exact(d)) engine = 3;
+    }
+    if (kw == 0) {
+      if (engine == t.engine) kw = t.stage_words;
+      else if (engine == 2) kw = t.rate_tc8 >= t.rate_tc4 ? 8 : 4;
+      else if (engine == 3) kw = t.rate_fp4_16 > t.rate_fp4_8 ? 16 : 8;
+    }
   }
-  if (engine == 2) return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts, kw);
+  if (engine == 2 && kw != 0 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
+  if (engine == 3 && kw != 0 && kw != 8 && kw != 16)
+    return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 8 or 16 with the FP4 engine");
+  if (engine == 2 || engine == 3)
+    return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts, kw, engine == 3);
+
   const int64_t n_first = std::max<int64_t>(ie - ib, 1);
   std::vector<int64_t> off((size_t)n_first + 1, 0);
   for (int64_t t = 0; t < n_first; t++) off[(size_t)t + 1] = off[(size_t)t] + (ib + t < ie ? groups_of(m, ib + t) : 0);
@@ -342,18 +359,20 @@ int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_
   return EPIK2_OK;
 }
 
-// Tensor-core engine: one CTA per SM, tiles = pair blocks (i, j0..j0+31) x k blocks of 128.
+// Tensor-core engine: one CTA per SM, tiles = pair blocks (i, j0..j0+31) x k blocks of
+// 128 (int8 format) or 112 (FP4 format) SNPs.
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
-                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw) {
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4) {
   const int64_t m = d.n_snps;
-  const int64_t n_kb = (m + 127) / 128;
+  const int64_t kk = tc_k_per_tile(fp4);
+  const int64_t n_kb = (m + kk - 1) / kk;
   std::vector<uint32_t> ij;
   std::vector<int64_t> off(1, 0);
   for (int64_t i = ib; i < ie; i++)
     for (int64_t j0 = i + 1; j0 <= m - 2; j0 += 32) {
       ij.push_back((uint32_t)i);
       ij.push_back((uint32_t)j0);
-      off.push_back(off.back() + (n_kb - (j0 + 1) / 128));
+      off.push_back(off.back() + (n_kb - (j0 + 1) / kk));
     }
   const int64_t n_pb = (int64_t)off.size() - 1;
   int r = ensure_pb(ctx, std::max<int64_t>(n_pb, 1));
@@ -391,7 +410,7 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   p.dump_scores = dump_scores;
   p.err = ctx->d_err;
   CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
-  CK(ctx, launch_scan_tc(p, ctx->tc_blocks, kw, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
+  CK(ctx, launch_scan_tc(p, ctx->tc_blocks, kw, fp4, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
   CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
   const int n_warps = ctx->tc_blocks * tc_warps_per_block();
   CK(ctx, launch_reduce_best(ctx->d_slots, n_warps, ctx->d_best, ctx->stream), "reduce kernel");
@@ -433,9 +452,11 @@ int autotune_now(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
   int64_t ie = 1;
   while (ie < m && (triplets_before(m, ie) * 64 < total || triplets_before(m, ie) < 4ll * ctx->tc_blocks * 4096)) ie++;
   const double ts = (double)triplets_before(m, ie) * (double)d.n_samples;
-  double rate[3] = {0, 0, 0};
-  const int eng[3] = {1, 2, 2}, kws[3] = {0, 4, 8};
-  for (int c = 0; c < 3; c++) {
+  // candidates: integer; int8 tensor cores, 4 or 8 words per stage; FP4 tensor cores, 8 or 16
+  double rate[5] = {0, 0, 0, 0, 0};
+  const int eng[5] = {1, 2, 2, 3, 3}, kws[5] = {0, 4, 8, 8, 16};
+  const int n_cand = fp4_exact(d) ? 5 : 3;
+  for (int c = 0; c < n_cand; c++) {
     epik2_opts o{};
     o.engine = eng[c];
     o.stage_words = kws[c];
@@ -452,8 +473,13 @@ int autotune_now(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
   t.rate_int = rate[0];
   t.rate_tc4 = rate[1];
   t.rate_tc8 = rate[2];
-  t.stage_words = rate[2] > rate[1] ? 8 : 4;
-  t.engine = std::max(rate[1], rate[2]) >= rate[0] ? 2 : 1;
+  t.rate_fp4_8 = rate[3];
+  t.rate_fp4_16 = rate[4];
+  int best = 0;
+  for (int c = 1; c < n_cand; c++)
+    if (rate[c] > rate[best]) best = c;
+  t.engine = eng[best];
+  t.stage_words = best == 0 ? (rate[2] > rate[1] ? 8 : 4) : kws[best];
   *out = t;
   return EPIK2_OK;
 }
@@ -481,10 +507,10 @@ int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
 // Batched form: build (or reuse) the plan for these datasets, refresh the job table from
 // the datasets' current class split, replay the captured launch sequence.
 int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vector<int32_t>& ids, int kw,
-              bool rescore, epik2_best* out) {
+              bool fp4, bool rescore, epik2_best* out) {
   std::vector<int64_t> key;
   for (const DevDataset* d : ds) key.push_back(d->n_snps);
-  key.push_back(kw * 2 + (rescore ? 1 : 0));
+  key.push_back(kw * 4 + (fp4 ? 2 : 0) + (rescore ? 1 : 0));
   BatchPlan* plan = nullptr;
   auto it = ctx->plans.find(key);
   const int32_t n = (int32_t)ds.size();
@@ -515,7 +541,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     };
     std::map<int64_t, ListInfo> lists;
     for (int32_t b = 0; b < n; b++) {
-      const int64_t m = ds[b]->n_snps, n_kb = (m + 127) / 128;
+      const int64_t m = ds[b]->n_snps, kk = tc_k_per_tile(fp4), n_kb = (m + kk - 1) / kk;
       auto li = lists.find(m);
       if (li == lists.end()) {
         ListInfo L{(int64_t)pb_off_all.size(), (int64_t)pb_ij_all.size(), 0, 0};
@@ -524,7 +550,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
           for (int64_t j0 = i + 1; j0 <= m - 2; j0 += 32) {
             pb_ij_all.push_back((uint32_t)i);
             pb_ij_all.push_back((uint32_t)j0);
-            L.tiles += n_kb - (j0 + 1) / 128;
+            L.tiles += n_kb - (j0 + 1) / kk;
             pb_off_all.push_back(L.tiles);
             L.n_pb++;
           }
@@ -574,7 +600,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     cudaError_t e = launch_fill_slots(pl->d_job_slots, (int64_t)n * grid, ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream);
-    if (e == cudaSuccess) e = launch_scan_tc(p, grid, kw, false, ctx->stream);
+    if (e == cudaSuccess) e = launch_scan_tc(p, grid, kw, fp4, false, ctx->stream);
     if (e == cudaSuccess) e = launch_reduce_jobs(pl->d_job_slots, n, grid, pl->d_results, ctx->stream);
     if (e == cudaSuccess && rescore) e = launch_rescore_jobs(pl->d_jobs, pl->d_results, n, pl->d_resc, ctx->stream);
     if (e == cudaSuccess && rescore)
@@ -734,7 +760,7 @@ int epik2_set_stream(epik2_ctx* ctx, void* cuda_stream) {
 
 int epik2_set_engine(epik2_ctx* ctx, int engine) {
   if (!ctx) return EPIK2_E_INVALID;
-  if (engine < EPIK2_ENGINE_AUTO || engine > EPIK2_ENGINE_TC) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
+  if (engine < EPIK2_ENGINE_AUTO || engine > EPIK2_ENGINE_TC_FP4) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
   ctx->engine = engine;
   return EPIK2_OK;
 }
@@ -1008,15 +1034,34 @@ int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, cons
       largest = d;
   }
   CK(ctx, cudaSetDevice(ctx->device), "set device");
+  // format: the requested tensor-core format, else the autotuner's choice for the largest
+  // dataset (int8 when it chose the integer engine or when a class is too large for FP4)
+  bool all_fp4 = true;
+  for (const DevDataset* d : ds) all_fp4 = all_fp4 && fp4_exact(*d);
+  int engine = opts ? opts->engine : 0;
+  if (engine == EPIK2_ENGINE_INT) return fail(ctx, EPIK2_E_INVALID, "the batched form runs on the tensor cores");
+  if (engine < 0 || engine > EPIK2_ENGINE_TC_FP4) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
+  if (engine == EPIK2_ENGINE_TC_FP4 && !all_fp4)
+    return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
   int kw = (opts && opts->stage_words) ? opts->stage_words : 0;
-  if (kw != 0 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
-  if (kw == 0) {
+  if (engine == 0 || kw == 0) {
     epik2_tune t{};
     int r = tuned(ctx, *largest, &t);
     if (r) return r;
-    kw = t.stage_words;
+    if (engine == 0) {  // a requested stage depth that only one format takes picks that format
+      engine = (t.engine == EPIK2_ENGINE_TC_FP4 && all_fp4) ? EPIK2_ENGINE_TC_FP4 : EPIK2_ENGINE_TC;
+      if (kw == 4) engine = EPIK2_ENGINE_TC;
+      if (kw == 16 && all_fp4) engine = EPIK2_ENGINE_TC_FP4;
+    }
+    if (kw == 0) {
+      if (engine == EPIK2_ENGINE_TC_FP4) kw = t.rate_fp4_16 > t.rate_fp4_8 ? 16 : 8;
+      else kw = t.rate_tc8 >= t.rate_tc4 ? 8 : 4;
+    }
   }
-  return run_batch(ctx, ds, ids, kw, opts && opts->rescore_fp64, out);
+  const bool fp4 = engine == EPIK2_ENGINE_TC_FP4;
+  if (!fp4 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
+  if (fp4 && kw != 8 && kw != 16) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 8 or 16 with the FP4 engine");
+  return run_batch(ctx, ds, ids, kw, fp4, opts && opts->rescore_fp64, out);
 }
 
 int epik2_dump_tables(epik2_ctx* ctx, int32_t dataset_id, uint32_t* tables, float* scores) {

@@ -126,7 +126,9 @@ cudaError_t launch_tables(const DevDataset& d, const uint32_t* triplets, int64_t
                           cudaStream_t stream);
 cudaError_t launch_rescore(const DevDataset& d, const BestSlot* cand, int64_t n, Rescored* out, cudaStream_t stream);
 int scan_blocks_per_sm();
-cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool dump, cudaStream_t stream);
+cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool dump,
+                           cudaStream_t stream);
+int tc_k_per_tile(bool fp4);  // SNPs k per tensor-core tile: 128 (int8) or 112 (FP4)
 cudaError_t launch_reduce_jobs(const BestSlot* slots, int n_jobs, int per_job, BestSlot* out, cudaStream_t stream);
 cudaError_t launch_fill_slots(BestSlot* slots, int64_t n, cudaStream_t stream);
 cudaError_t tc_configure();

@@ -38,13 +38,19 @@ namespace epik2 {
 constexpr int kTcThreads = 512;  // 16 operand-producing / epilogue warps
 constexpr int kTcWarps = kTcThreads / 32;
 constexpr int kTcThreadsAll = kTcThreads + 32;  // + one warp that only issues the MMAs
-constexpr int kTcK = 128;        // SNPs k per tile  -> 256 rows of B
 constexpr int kRingBytes = 16 * 384 * 32;  // stage ring: kStages x 384 rows x (32 * kW) bytes = 192 KiB
 constexpr int kTcSmemBytes = kRingBytes + 256;  // + mbarriers
 constexpr int kEStride = 129;  // words per row of the epilogue staging buffer
 constexpr long long kWaitLimit = 4000000000LL;  // SM clocks (~2 s) before a wait gives up
 // instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = 256, M = 128
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+// block-scaled instruction descriptor (kind::mxf4): A/B E2M1, scale factors UE8M0, both
+// K-major, N = 224, M = 128, K = 64, scale-factor byte selectors 0.  D is FP32.
+constexpr uint32_t kIdescFp4 = (1u << 7) | (1u << 10) | ((224u >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
+// FP4 format: TMEM columns [224, 256) hold the scale factors (all 2^1), A's from 224 (4
+// columns), B's from 240 (8 columns); class 0 accumulates into [0, 224), class 1 into
+// [256, 480).
+constexpr uint32_t kSfaCol = 224, kSfbCol = 240;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
   return (uint32_t)__cvta_generic_to_shared(ptr);
@@ -64,6 +70,27 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, 
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
       "l"(a), "l"(b), "r"(kIdescI8), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
+
+// One block-scaled FP4 MMA: operands 0 or 0.5 (E2M1 0b0001), every scale factor 2, so each
+// product is 0 or 1 and the FP32 sums are exact counts (below 2^24 per class).
+__device__ __forceinline__ void mma_fp4(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate,
+                                        uint32_t sfa_tmem, uint32_t sfb_tmem) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.scale_vec::2X [%0], %1, %2, %3, [%5], [%6], p;\n\t}\n" ::"r"(
+          d_tmem),
+      "l"(a), "l"(b), "r"(kIdescFp4), "r"(accumulate), "r"(sfa_tmem), "r"(sfb_tmem));
+}
+
+__device__ __forceinline__ void tmem_st16_fill(uint32_t addr, uint32_t v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+      "%1};" ::"r"(addr),
+      "r"(v)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -135,6 +162,13 @@ __device__ __forceinline__ uint4 expand16(uint32_t h) {
   return r;
 }
 
+// 32 sample bits -> 16 bytes of E2M1 operands, 0 (absent) or 0.5 (present, nibble 0b0001):
+// 32-bit word q of the group holds samples q, q+4, ..., q+28 in its eight nibbles.  The same
+// order is used for A and B.
+__device__ __forceinline__ uint4 expand32_fp4(uint32_t w) {
+  return make_uint4(w & 0x11111111u, (w >> 1) & 0x11111111u, (w >> 2) & 0x11111111u, (w >> 3) & 0x11111111u);
+}
+
 __device__ __forceinline__ void sts128(uint32_t saddr, uint4 v) {
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(saddr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
                : "memory");
@@ -153,15 +187,22 @@ struct JobView {
   int32_t m, m_pad, w0, w1, n0, n1;
 };
 
-// kW = class words (32 samples each) per pipeline stage: 4 (4 stages of 48 KiB) or 8 (2
-// stages of 96 KiB).  kBatched: tiles of many datasets on one queue, per-dataset results.
-template <int kW, bool kBatched, bool kDump, bool kTopK>
+// kFp4 selects the operand format: int8 (kind::i8, 128 SNPs k per tile, kW = 4 or 8 words
+// per stage: 4 stages of 48 KiB or 2 of 96 KiB) or E2M1 (kind::mxf4, 112 SNPs k per tile so
+// that the scale factors fit in tensor memory beside the two accumulators, kW = 8 or 16:
+// 4 stages of 44 KiB or 2 of 88 KiB).  kW = class words (32 samples each) per stage.
+// kBatched: tiles of many datasets on one queue, per-dataset results.
+template <int kW, bool kFp4, bool kBatched, bool kDump, bool kTopK>
 __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) {
-  constexpr int kStages = 16 / kW;
-  constexpr int kStageA = 128 * 32 * kW;            // bytes: 128 rows x 32*kW samples
-  constexpr int kStageBytes = 384 * 32 * kW;        // A + B (256 rows)
-  constexpr uint32_t kSbo = 256 * kW;               // bytes between 8-row groups
-  constexpr int kU = kW / 4;                        // units of each kind per thread per stage
+  constexpr int kK = kFp4 ? 112 : 128;                // SNPs k per tile -> 2*kK rows of B
+  constexpr int kRowBytes = (kFp4 ? 16 : 32) * kW;    // operand bytes per row per stage
+  constexpr int kStageA = 128 * kRowBytes;
+  constexpr int kStageBytes = (128 + 2 * kK) * kRowBytes;
+  constexpr int kStages = kRingBytes / kStageBytes;
+  constexpr uint32_t kSbo = 8 * kRowBytes;            // bytes between 8-row groups
+  constexpr int kMmas = kFp4 ? kW / 2 : kW;           // MMAs per stage (K = 64 E2M1 or 32 int8)
+  constexpr int kU = kW / 4;                          // units of each kind per thread per stage
+  static_assert(kStages >= 2 && kStages <= 4, "stage ring");
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t s_tmem;
   __shared__ long long s_tile;
@@ -194,6 +235,17 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
+  if (kFp4) {  // scale factors: every byte of columns [224, 256) = 0x80 (2^1), all 128 lanes
+    if (warp < 4) {
+      const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + kSfaCol;
+      tmem_st16_fill(ta, 0x80808080u);
+      tmem_st16_fill(ta + 16, 0x80808080u);
+      tmem_wait_st();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
 
   float best_s = FLT_MAX;
   unsigned long long best_k = ~0ull;
@@ -235,20 +287,21 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       else hi = mid;
     }
     const int i = (int)jv.pb_ij[2 * lo], j0 = (int)jv.pb_ij[2 * lo + 1];
-    const int k0 = kTcK * ((j0 + 1) / kTcK + (int)(tile - jv.pb_off[lo]));
+    const int k0 = kK * ((j0 + 1) / kK + (int)(tile - jv.pb_off[lo]));
 
     // ---- operand expansion and MMA, 32*kW samples per stage ----
     // Units of a stage, kU of each kind per thread (r < kU):
     //   A: word w = (tid>>7) + 4r, row = tid&127 = 32*ab + q (pair q, g_i = ab>>1, g_j = ab&1)
-    //   B: word w = (tid>>7) + 4r, kl = tid&127 -> rows 128*c + kl (g_k = c) of both c
+    //   B: word w = (tid>>7) + 4r, kl = tid&127 (< kK) -> rows kK*c + kl (g_k = c) of both c
     // A warp writes 32 consecutive rows of one 16-byte K group per store (conflict-free).
     // The words of stage cc+1 are loaded while stage cc is expanded.
     const int a_row = tid & 127, a_ab = a_row >> 5, w_base = tid >> 7;
     const int a_j = min(j0 + (a_row & 31), (int)m_pad - 1);
     const int b_kl = tid & 127;
+    const bool b_on = b_kl < kK;
     const int b_k = k0 + b_kl;
     const uint32_t offa0 = (a_row >> 3) * kSbo + (a_row & 7) * 16;
-    const uint32_t offb0 = (b_kl >> 3) * kSbo + (b_kl & 7) * 16;  // + 128*kSbo/8 for c = 1
+    const uint32_t offb0 = (b_kl >> 3) * kSbo + (b_kl & 7) * 16;  // + (kK/8)*kSbo for c = 1
     auto load_words = [&](int cc, uint2 (&gi)[kU], uint2 (&gj)[kU], uint2 (&gk)[kU]) {
       const bool c1 = cc >= nc0;
       const int c_in = c1 ? cc - nc0 : cc;
@@ -264,7 +317,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
           const uint2* row = jv.planes + (wb + w) * m_pad;
           gi[r] = __ldg(row + i);
           gj[r] = __ldg(row + a_j);
-          if (b_k < m_pad) gk[r] = __ldg(row + b_k);
+          if (b_on && b_k < m_pad) gk[r] = __ldg(row + b_k);
         }
       }
     };
@@ -287,14 +340,23 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         for (int r = 0; r < kU; r++) {
           const int w = w_base + 4 * r;
           const uint32_t wa = ((a_ab >> 1) ? ci[r].y : ci[r].x) & ((a_ab & 1) ? cj[r].y : cj[r].x);
-          const uint32_t offa = sA + offa0 + (2 * w) * 128;
-          sts128(offa, expand16(wa));
-          sts128(offa + 128, expand16(wa >> 16));
-          const uint32_t offb = sB + offb0 + (2 * w) * 128;
-          sts128(offb, expand16(ck[r].x));
-          sts128(offb + 128, expand16(ck[r].x >> 16));
-          sts128(offb + 16 * kSbo, expand16(ck[r].y));
-          sts128(offb + 16 * kSbo + 128, expand16(ck[r].y >> 16));
+          if (kFp4) {  // word w = K group w (16 bytes)
+            sts128(sA + offa0 + w * 128, expand32_fp4(wa));
+            if (b_on) {
+              const uint32_t offb = sB + offb0 + w * 128;
+              sts128(offb, expand32_fp4(ck[r].x));
+              sts128(offb + (kK / 8) * kSbo, expand32_fp4(ck[r].y));
+            }
+          } else {  // word w = K groups 2w, 2w+1
+            const uint32_t offa = sA + offa0 + (2 * w) * 128;
+            sts128(offa, expand16(wa));
+            sts128(offa + 128, expand16(wa >> 16));
+            const uint32_t offb = sB + offb0 + (2 * w) * 128;
+            sts128(offb, expand16(ck[r].x));
+            sts128(offb + 128, expand16(ck[r].x >> 16));
+            sts128(offb + (kK / 8) * kSbo, expand16(ck[r].y));
+            sts128(offb + (kK / 8) * kSbo + 128, expand16(ck[r].y >> 16));
+          }
         }
 #pragma unroll
         for (int r = 0; r < kU; r++) {
@@ -323,8 +385,13 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         const uint32_t d = tmem + (c1 ? 256u : 0u);
         const uint64_t da = smem_desc(sA, kSbo), db = smem_desc(sB, kSbo);
 #pragma unroll
-        for (int kk = 0; kk < kW; kk++)
-          mma_i8(d, da + (uint64_t)(16 * kk), db + (uint64_t)(16 * kk), (c_in > 0 || kk > 0) ? 1u : 0u);
+        for (int kk = 0; kk < kMmas; kk++) {  // each MMA reads 32 bytes of every row: 256 B on
+          const uint32_t acc = (c_in > 0 || kk > 0) ? 1u : 0u;
+          if (kFp4)
+            mma_fp4(d, da + (uint64_t)(16 * kk), db + (uint64_t)(16 * kk), acc, tmem + kSfaCol, tmem + kSfbCol);
+          else
+            mma_i8(d, da + (uint64_t)(16 * kk), db + (uint64_t)(16 * kk), acc);
+        }
         mma_commit(bar0 + 8 * s);
         if (cc == nct - 1) mma_commit(bar_acc);
       }
@@ -343,9 +410,10 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     }
     tc_fence_after();
     ++n_tile;
-    // Accumulator layout: TMEM lane = 32*ab + q, column = 128*c + kl (per class: +256*cls).
-    // Per half h (kl in [64h, 64h+64)) each warp copies lanes 32*(warp&3).. and 32 columns
-    // of both c into E[cls][lane][64*c + kl - 64h] (row stride kEStride words).
+    // Accumulator layout: TMEM lane = 32*ab + q, column = kK*c + kl (per class: +256*cls).
+    // Per half h (kl in [64h, min(64h+64, kK))) each warp copies lanes 32*(warp&3).. and up
+    // to 32 columns of both c into E[cls][lane][64*c + kl - 64h] (row stride kEStride
+    // words); FP32 accumulators (FP4 format) are converted to the integer counts they hold.
     const int quarter = warp & 3, cgrp = warp >> 2;
     const int row = 32 * quarter + lane;
     const int e_c = cgrp >> 1, e_sub = cgrp & 1;
@@ -359,11 +427,16 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         const bool has = (cls ? nc1 > 0 : nc0 > 0) && worker;
 #pragma unroll
         for (int part = 0; part < 2; part++) {
-          const int col = 128 * e_c + 64 * h + 32 * e_sub + 16 * part;  // inside the class accumulator
+          const int kin = 64 * h + 32 * e_sub + 16 * part;  // first k of the 16 columns
+          const int col = kK * e_c + kin;                     // inside the class accumulator
           uint32_t v[16];
-          if (has) {
+          if (has && kin < kK) {  // warp-uniform
             tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(cls * 256 + col), v);
             tmem_wait_ld();
+            if (kFp4) {
+#pragma unroll
+              for (int t = 0; t < 16; t++) v[t] = __float2uint_rn(__uint_as_float(v[t]));
+            }
           } else {
 #pragma unroll
             for (int t = 0; t < 16; t++) v[t] = 0;
@@ -384,7 +457,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         const int kl = x & 63, q = x >> 6;
         const int j = j0 + q;
         const int k = k0 + 64 * h + kl;
-        const bool valid = (j < m) && (k > j) && (k < m);
+        const bool valid = (64 * h + kl < kK) && (j < m) && (k > j) && (k < m);
         float sc = FLT_MAX;
         unsigned long long key = ~0ull;
         if (valid) {
@@ -563,43 +636,56 @@ __global__ void k_fill_slots(BestSlot* __restrict__ slots, int64_t n) {
 
 int tc_warps_per_block() { return kTcWarps; }
 
-template <int kW, bool kB, bool kD, bool kT>
+template <int kW, bool kF, bool kB, bool kD, bool kT>
 static cudaError_t set_smem() {
-  return cudaFuncSetAttribute(k_scan_tc<kW, kB, kD, kT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
+  return cudaFuncSetAttribute(k_scan_tc<kW, kF, kB, kD, kT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kTcSmemBytes);
+}
+
+template <int kW, bool kF>
+static cudaError_t set_smem_all() {
+  cudaError_t e = set_smem<kW, kF, false, false, false>();
+  if (e == cudaSuccess) e = set_smem<kW, kF, false, true, false>();
+  if (e == cudaSuccess) e = set_smem<kW, kF, false, false, true>();
+  if (e == cudaSuccess) e = set_smem<kW, kF, true, false, false>();
+  return e;
 }
 
 cudaError_t tc_configure() {
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = set_smem<4, false, false, false>();
-    if (e == cudaSuccess) e = set_smem<4, false, true, false>();
-    if (e == cudaSuccess) e = set_smem<4, false, false, true>();
-    if (e == cudaSuccess) e = set_smem<8, false, false, false>();
-    if (e == cudaSuccess) e = set_smem<8, false, true, false>();
-    if (e == cudaSuccess) e = set_smem<8, false, false, true>();
-    if (e == cudaSuccess) e = set_smem<4, true, false, false>();
-    if (e == cudaSuccess) e = set_smem<8, true, false, false>();
+    cudaError_t e = set_smem_all<4, false>();
+    if (e == cudaSuccess) e = set_smem_all<8, false>();
+    if (e == cudaSuccess) e = set_smem_all<8, true>();
+    if (e == cudaSuccess) e = set_smem_all<16, true>();
     if (e != cudaSuccess) return e;
     configured = true;
   }
   return cudaSuccess;
 }
 
-cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool dump, cudaStream_t stream) {
+template <int kW, bool kF>
+static void launch_variant(const TcParams& p, int blocks, bool batched, bool dump, bool topk, cudaStream_t stream) {
+  if (batched) k_scan_tc<kW, kF, true, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+  else if (dump) k_scan_tc<kW, kF, false, true, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+  else if (topk) k_scan_tc<kW, kF, false, false, true><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+  else k_scan_tc<kW, kF, false, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+}
+
+int tc_k_per_tile(bool fp4) { return fp4 ? 112 : 128; }
+
+cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool dump,
+                           cudaStream_t stream) {
   const cudaError_t ce = tc_configure();
   if (ce != cudaSuccess) return ce;
   const bool topk = p.top_k > 1;
   const bool batched = p.jobs != nullptr;
-  if (words_per_stage == 8) {
-    if (batched) k_scan_tc<8, true, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
-    else if (dump) k_scan_tc<8, false, true, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
-    else if (topk) k_scan_tc<8, false, false, true><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
-    else k_scan_tc<8, false, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+  if (fp4) {
+    if (words_per_stage == 16) launch_variant<16, true>(p, blocks, batched, dump, topk, stream);
+    else launch_variant<8, true>(p, blocks, batched, dump, topk, stream);
   } else {
-    if (batched) k_scan_tc<4, true, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
-    else if (dump) k_scan_tc<4, false, true, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
-    else if (topk) k_scan_tc<4, false, false, true><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
-    else k_scan_tc<4, false, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+    if (words_per_stage == 8) launch_variant<8, false>(p, blocks, batched, dump, topk, stream);
+    else launch_variant<4, false>(p, blocks, batched, dump, topk, stream);
   }
   return cudaGetLastError();
 }

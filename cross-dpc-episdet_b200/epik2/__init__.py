@@ -32,6 +32,7 @@ E_CANCELLED = -9
 ENGINE_AUTO = 0
 ENGINE_INT = 1
 ENGINE_TC = 2
+ENGINE_TC_FP4 = 3
 
 
 class Epik2Error(RuntimeError):
@@ -63,7 +64,8 @@ class Stats(ctypes.Structure):
 
 class Tune(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("rate_int", ctypes.c_double),
-                ("rate_tc4", ctypes.c_double), ("rate_tc8", ctypes.c_double)]
+                ("rate_tc4", ctypes.c_double), ("rate_tc8", ctypes.c_double), ("rate_fp4_8", ctypes.c_double),
+                ("rate_fp4_16", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -69,11 +69,13 @@ typedef struct {
 
 /* Scan options.  Zero-initialise and set what you need; 0 means "default". */
 typedef struct {
-  int32_t engine;      /* 0 = the context's default, 1 = integer pipe (LOP3+POPC), 2 = tensor cores */
+  int32_t engine;      /* 0 = the context's default, 1 = integer pipe (LOP3+POPC), 2 = tensor cores
+                          (int8), 3 = tensor cores (block-scaled FP4) */
   int32_t top_k;       /* 0/1 = best only; >1 = keep the top_k lowest FP32 scores */
   int32_t rescore_fp64;/* 1 = rescore the kept candidates in FP64 on the GPU */
   int32_t k_strip;     /* tuning: SNPs per k-strip (multiple of 32); 0 = autotuned */
-  int32_t stage_words;  /* tuning, tensor cores: 32-sample words per pipeline stage, 4 or 8; 0 = autotuned */
+  int32_t stage_words;  /* tuning, tensor cores: 32-sample words per pipeline stage, 4 or 8 (int8),
+                           8 or 16 (FP4); 0 = autotuned */
   int32_t blocks_per_sm;  /* tuning: 0 = occupancy-derived */
   int64_t snp_begin;   /* restrict the first index i to [snp_begin, snp_end); 0,0 = all */
   int64_t snp_end;
@@ -91,11 +93,14 @@ int epik2_device_name(const epik2_ctx *ctx, char *buf, size_t len);
 /* Bytes of device memory currently free / total on the context's device. */
 int epik2_mem_info(const epik2_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
 
-/* Default search engine of the context (EPIK2_ENGINE_*).  Both engines give identical
- * tables, scores and triplets; AUTO is the tensor-core engine. */
+/* Default search engine of the context (EPIK2_ENGINE_*).  All engines give identical
+ * tables, scores and triplets; AUTO takes the autotuner's choice for the dataset's shape. */
 #define EPIK2_ENGINE_AUTO 0
 #define EPIK2_ENGINE_INT 1 /* integer pipe: 8 LOP3+POPC per triplet and 32-sample word */
 #define EPIK2_ENGINE_TC 2  /* tcgen05 int8 matrix products on 0/1 operands, int32 accumulators */
+#define EPIK2_ENGINE_TC_FP4 3 /* tcgen05 block-scaled FP4 (E2M1 0/0.5, scales 2) products, FP32
+                                 accumulators: exact while every class has < 2^24 samples,
+                                 else EPIK2_E_TOO_LARGE */
 int epik2_set_engine(epik2_ctx *ctx, int engine);
 
 /* Run the context's work on a caller-owned stream (e.g. a PyTorch stream); NULL restores
@@ -180,17 +185,20 @@ int epik2_scan_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int
 int epik2_scan_batch(epik2_ctx *ctx, const int32_t *dataset_ids, int32_t n, const epik2_opts *opts,
                      epik2_best *out);
 
-/* Autotuner (no reference counterpart).  Times the integer engine and the tensor-core
- * engine at 4 and 8 words per stage on a slice of the dataset (about 1/64 of its
- * triplets, at least a few tiles per SM) and caches the fastest per shape bucket
- * (log2 of samples and SNPs); EPIK2_ENGINE_AUTO scans use the cached choice.  Reports the
- * choice and the measured rates (triplet*samples/s) of the three candidates. */
+/* Autotuner (no reference counterpart).  Times the integer engine, the int8 tensor-core
+ * engine at 4 and 8 words per stage and the FP4 tensor-core engine at 8 and 16 words per
+ * stage (when its accumulators are exact for the dataset) on a slice of the dataset
+ * (about 1/64 of its triplets, at least a few tiles per SM) and caches the fastest per
+ * shape bucket (log2 of samples and SNPs); EPIK2_ENGINE_AUTO scans use the cached choice.
+ * Reports the choice and the measured rates (triplet*samples/s; 0 = not a candidate). */
 typedef struct {
-  int32_t engine;        /* EPIK2_ENGINE_INT or EPIK2_ENGINE_TC */
-  int32_t stage_words;   /* tensor-core stage depth chosen (4 or 8) */
+  int32_t engine;        /* EPIK2_ENGINE_INT, EPIK2_ENGINE_TC or EPIK2_ENGINE_TC_FP4 */
+  int32_t stage_words;   /* tensor-core stage depth chosen (int8: 4 or 8, FP4: 8 or 16) */
   double rate_int;       /* measured rates on the slice */
   double rate_tc4;
   double rate_tc8;
+  double rate_fp4_8;
+  double rate_fp4_16;
 } epik2_tune;
 int epik2_autotune(epik2_ctx *ctx, int32_t dataset_id, epik2_tune *out);
 

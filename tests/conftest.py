@@ -56,12 +56,13 @@ def pytest_collection_modifyitems(config, items):
             item.add_marker(skip)
 
 
-ENGINES = {1: "int", 2: "tc"}
+ENGINES = {1: "int", 2: "tc", 3: "fp4"}
 
 
-@pytest.fixture(scope="session", params=[1, 2], ids=["int", "tc"])
+@pytest.fixture(scope="session", params=[1, 2, 3], ids=["int", "tc", "fp4"])
 def ctx(request):
-    """A device context per search engine: every test that takes `ctx` runs on both."""
+    """A device context per search engine (integer pipe, int8 tensor cores, FP4 tensor
+    cores): every test that takes `ctx` runs on all three."""
     import epik2
     c = epik2.Context(0, engine=request.param)
     yield c

@@ -16,14 +16,15 @@ MIXED = [  # (seed, samples, SNPs, cases): uneven sizes, class splits and tile c
 ]
 
 
-@pytest.mark.parametrize("stage_words", [4, 8])
-def test_batch_equals_separate_runs_and_oracle(stage_words):
+@pytest.mark.parametrize("engine,stage_words", [(2, 4), (2, 8), (3, 8), (3, 16)],
+                         ids=["tc-4", "tc-8", "fp4-8", "fp4-16"])
+def test_batch_equals_separate_runs_and_oracle(engine, stage_words):
     data = [O.gen_hwe(sd, S, M, c) for sd, S, M, c in MIXED]
     with epik2.Context(0) as ctx:
         ids = [ctx.load(g, p) for g, p in data]
-        batched = ctx.scan_batch(ids, stage_words=stage_words)
-        again = ctx.scan_batch(ids, stage_words=stage_words)  # graph replay
-        single = [ctx.scan(d, engine=epik2.ENGINE_TC, stage_words=stage_words) for d in ids]
+        batched = ctx.scan_batch(ids, engine=engine, stage_words=stage_words)
+        again = ctx.scan_batch(ids, engine=engine, stage_words=stage_words)  # graph replay
+        single = [ctx.scan(d, engine=engine, stage_words=stage_words) for d in ids]
         single_int = [ctx.scan(d, engine=epik2.ENGINE_INT) for d in ids]
     for (g, p), b, b2, s, si in zip(data, batched, again, single, single_int):
         ref = O.scan(g, p) if g.shape[1] <= 140 else None
@@ -68,8 +69,26 @@ def test_autotune_reports_all_candidates():
         d = ctx.load(g, p)
         t = ctx.autotune(d)
         b = ctx.scan(d)  # AUTO engine uses the cached choice
-    assert t["engine"] in (epik2.ENGINE_INT, epik2.ENGINE_TC)
-    assert t["stage_words"] in (4, 8)
-    assert min(t["rate_int"], t["rate_tc4"], t["rate_tc8"]) > 0
+    assert t["engine"] in (epik2.ENGINE_INT, epik2.ENGINE_TC, epik2.ENGINE_TC_FP4)
+    assert t["stage_words"] in ((8, 16) if t["engine"] == epik2.ENGINE_TC_FP4 else (4, 8))
+    assert min(t["rate_int"], t["rate_tc4"], t["rate_tc8"], t["rate_fp4_8"], t["rate_fp4_16"]) > 0
     r = O.scan(g, p)
     assert b.ijk == r["ijk"]
+
+
+def test_fp4_refuses_classes_of_2_24_samples():
+    """FP32 accumulators hold exact counts below 2^24 per class: the FP4 engine refuses a
+    larger class; the int8 engine (int32 accumulators) and the autotuner's choice serve it."""
+    n = (1 << 24) + 64
+    rng = np.random.default_rng(9)
+    g = rng.integers(0, 3, size=(n, 3), dtype=np.uint8)
+    p = np.zeros(n, dtype=np.uint8)
+    p[:64] = 1  # 2^24 controls
+    with epik2.Context(0) as ctx:
+        d = ctx.load(g, p)
+        with pytest.raises(epik2.Epik2Error) as e:
+            ctx.scan(d, engine=epik2.ENGINE_TC_FP4)
+        assert e.value.status == epik2.E_TOO_LARGE
+        b8 = ctx.scan(d, engine=epik2.ENGINE_TC)
+        bi = ctx.scan(d, engine=epik2.ENGINE_INT)
+    assert b8.ijk == bi.ijk == (0, 1, 2) and f32_bits(b8.score) == f32_bits(bi.score)
