@@ -193,7 +193,8 @@ def run_ours(args, rank, world, local_rank):
     shards = SH.shard_bounds(M, parts)
     peaks = epik2.probe_int_peaks(local_rank)
     tune = ctx.autotune(did)  # AUTO-engine scans below use this choice
-    engine_tc = tune["engine"] == epik2.ENGINE_TC
+    engine_tc = tune["engine"] in (epik2.ENGINE_TC, epik2.ENGINE_TC_FP4)
+    engine_fp4 = tune["engine"] == epik2.ENGINE_TC_FP4
     flush = torch.empty(args.flush_mb << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
 
     def shard_of(t):
@@ -269,11 +270,15 @@ def run_ours(args, rank, world, local_rank):
             traffic = tr["dram_bytes_per_triplet"] * sum(step_trip) / len(step_trip)
     except (OSError, KeyError, ValueError):
         pass
-    if engine_tc and "tc_i8_mac_per_s" in peaks:
+    peak_key = "tc_fp4_mac_per_s" if engine_fp4 else "tc_i8_mac_per_s"
+    if engine_tc and peak_key in peaks:
+        # 8 counted cells per triplet and sample = 8 multiply-accumulates = 16 operations
         ops = 16.0 * ts_local / kernel_s
-        roof = {"bound": "tensor", "achieved": ops / 1e12, "peak": 2 * peaks["tc_i8_mac_per_s"] / 1e12,
-                "unit": "TOPS (int8)", "frac": ops / (2 * peaks["tc_i8_mac_per_s"]),
-                "peak_source": "measured live by epik2_probe_tc_i8 on this GPU (dense tcgen05 kind::i8)",
+        roof = {"bound": "tensor", "achieved": ops / 1e12, "peak": 2 * peaks[peak_key] / 1e12,
+                "unit": "TOPS (fp4)" if engine_fp4 else "TOPS (int8)", "frac": ops / (2 * peaks[peak_key]),
+                "peak_source": ("measured live by epik2_probe_tc_fp4 on this GPU (dense tcgen05 kind::mxf4, "
+                                "M128 N224 K64)" if engine_fp4 else
+                                "measured live by epik2_probe_tc_i8 on this GPU (dense tcgen05 kind::i8)"),
                 "algorithmic_ops_per_triplet_sample": 16}
     else:
         roof = {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": peaks["popc_per_s"] / 1e9,
@@ -342,9 +347,12 @@ def run_ours(args, rank, world, local_rank):
                        "n_cases": info["n_cases"], "step": f"1/{parts} of the triplet space (first-index shard)",
                        "l2": f"flushed before every step ({args.flush_mb} MiB write)",
                        "parallelism": f"{world} GPU(s), shard-parallel",
-                       "engine": ("tensor cores (tcgen05 int8), %d words per stage" % tune["stage_words"]) if engine_tc
+                       "engine": ("tensor cores (tcgen05 %s), %d words per stage"
+                                  % ("block-scaled FP4" if engine_fp4 else "int8", tune["stage_words"])) if engine_tc
                        else "integer (LOP3+POPC)",
-                       "autotune_rates": {"int": tune["rate_int"], "tc4": tune["rate_tc4"], "tc8": tune["rate_tc8"]}},
+                       "autotune_rates": {"int": tune["rate_int"], "tc_int8_4": tune["rate_tc4"],
+                                          "tc_int8_8": tune["rate_tc8"], "tc_fp4_8": tune["rate_fp4_8"],
+                                          "tc_fp4_16": tune["rate_fp4_16"]}},
             "roofline": roof,
             "clocks": clocks,
             "gpu_launches": launches,

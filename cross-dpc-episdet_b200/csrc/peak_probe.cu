@@ -60,9 +60,12 @@ __global__ void k_iadd(uint32_t* out, int iters, uint32_t seed) {
   out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
-// Back-to-back tcgen05.mma kind::i8 M128 N256 K32 from zeroed shared memory (no-swizzle
-// K-major descriptors, LBO 128 B, SBO 1024 B), 512 tensor-memory columns per CTA.
+// Back-to-back tcgen05.mma from zeroed shared memory (no-swizzle K-major descriptors, LBO
+// 128 B, SBO 1024 B), 512 tensor-memory columns per CTA: kind::i8 M128 N256 K32, or the
+// search kernel's block-scaled FP4 shape kind::mxf4 M128 N224 K64 with its scale factors
+// (every byte 2^1) in columns [224, 256).  Accumulators alternate between columns 0 and 256.
 constexpr uint32_t kIdescProbe = (2u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kIdescProbeFp4 = (1u << 7) | (1u << 10) | ((224u >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
 constexpr int kProbeSmem = 153600;  // > half an SM's shared memory: one CTA per SM
 
 __device__ __forceinline__ uint64_t probe_desc(uint32_t saddr) {
@@ -70,7 +73,8 @@ __device__ __forceinline__ uint64_t probe_desc(uint32_t saddr) {
          ((uint64_t)1 << 46);
 }
 
-__global__ void __launch_bounds__(128, 1) k_tc_i8(int n_mma, int* err) {
+template <bool kFp4>
+__global__ void __launch_bounds__(128, 1) k_tc_probe(int n_mma, int* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t s_tmem;
   __shared__ __align__(8) uint64_t bar;
@@ -94,15 +98,35 @@ __global__ void __launch_bounds__(128, 1) k_tc_i8(int n_mma, int* err) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
+  if (kFp4) {  // scale factors: columns [224, 256) of the warp's 32 lanes
+    const uint32_t ta = tmem + ((uint32_t)(32 * (tid >> 5)) << 16) + 224u, v = 0x80808080u;
+#pragma unroll
+    for (int c = 0; c < 32; c += 16)
+      asm volatile(
+          "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+          "%1, %1};" ::"r"(ta + c),
+          "r"(v)
+          : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
   if (tid == 0) {
     for (int q = 0; q < n_mma; q++) {
       const int kk = q & 3;
-      asm volatile(
-          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-          "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-              tmem + ((q >> 2) & 1) * 256),
-          "l"(probe_desc(sbase + kk * 256)), "l"(probe_desc(sbase + 16384 + kk * 256)), "r"(kIdescProbe),
-          "r"(q > 1 ? 1u : 0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      const uint32_t d = tmem + ((q >> 2) & 1) * 256;
+      const uint64_t a = probe_desc(sbase + kk * 256), b = probe_desc(sbase + 16384 + kk * 256);
+      if (kFp4)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.scale_vec::2X [%0], %1, %2, %3, [%5], [%6], p;\n\t}\n" ::"r"(d),
+            "l"(a), "l"(b), "r"(kIdescProbeFp4), "r"(q > 1 ? 1u : 0u), "r"(tmem + 224u), "r"(tmem + 240u));
+      else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+            "l"(a), "l"(b), "r"(kIdescProbe), "r"(q > 1 ? 1u : 0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
     }
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(sbar) : "memory");
     uint32_t ok = 0;
@@ -168,7 +192,10 @@ extern "C" int epik2_probe_int_peaks(int device, double* popc_per_s, double* lop
   return r;
 }
 
-extern "C" int epik2_probe_tc_i8(int device, double* mac_per_s) {
+namespace {
+
+template <bool kFp4>
+int probe_tc(int device, double* mac_per_s) {
   if (!mac_per_s) return -1;
   if (cudaSetDevice(device) != cudaSuccess) return -7;
   int sms = 0;
@@ -176,7 +203,8 @@ extern "C" int epik2_probe_tc_i8(int device, double* mac_per_s) {
   int* d_err = nullptr;
   if (cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) return -3;
   cudaMemset(d_err, 0, sizeof(int));
-  if (cudaFuncSetAttribute(k_tc_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, kProbeSmem) != cudaSuccess) {
+  if (cudaFuncSetAttribute(k_tc_probe<kFp4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kProbeSmem) !=
+      cudaSuccess) {
     cudaFree(d_err);
     return -2;
   }
@@ -184,9 +212,9 @@ extern "C" int epik2_probe_tc_i8(int device, double* mac_per_s) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  k_tc_i8<<<sms, 128, kProbeSmem>>>(1024, d_err);
+  k_tc_probe<kFp4><<<sms, 128, kProbeSmem>>>(1024, d_err);
   cudaEventRecord(e0);
-  k_tc_i8<<<sms, 128, kProbeSmem>>>(n_mma, d_err);
+  k_tc_probe<kFp4><<<sms, 128, kProbeSmem>>>(n_mma, d_err);
   cudaEventRecord(e1);
   int r = cudaEventSynchronize(e1) == cudaSuccess ? 0 : -2;
   float ms = 0;
@@ -198,6 +226,13 @@ extern "C" int epik2_probe_tc_i8(int device, double* mac_per_s) {
   cudaFree(d_err);
   if (r) return r;
   if (herr) return -6;
-  *mac_per_s = (double)n_mma * 128.0 * 256.0 * 32.0 * sms / (ms * 1e-3);
+  const double macs_per_mma = kFp4 ? 128.0 * 224.0 * 64.0 : 128.0 * 256.0 * 32.0;
+  *mac_per_s = (double)n_mma * macs_per_mma * sms / (ms * 1e-3);
   return 0;
 }
+
+}  // namespace
+
+extern "C" int epik2_probe_tc_i8(int device, double* mac_per_s) { return probe_tc<false>(device, mac_per_s); }
+
+extern "C" int epik2_probe_tc_fp4(int device, double* mac_per_s) { return probe_tc<true>(device, mac_per_s); }

@@ -390,7 +390,8 @@ class Context:
 
 
 def probe_int_peaks(device=0):
-    """Measured POPC / LOP3 / IADD rates of the device, operations per second."""
+    """Measured POPC / LOP3 / IADD rates of the device (operations per second) and the dense
+    int8 and FP4 tensor-core rates (multiply-accumulates per second)."""
     if not os.path.exists(PROBE_LIB_PATH):
         raise Epik2Error(E_NO_DEVICE, f"{PROBE_LIB_PATH} not built")
     L = ctypes.CDLL(PROBE_LIB_PATH)
@@ -407,6 +408,10 @@ def probe_int_peaks(device=0):
     m = ctypes.c_double()
     if L.epik2_probe_tc_i8(device, ctypes.byref(m)) == 0:
         out["tc_i8_mac_per_s"] = m.value
+    L.epik2_probe_tc_fp4.argtypes = [ctypes.c_int, d]
+    L.epik2_probe_tc_fp4.restype = ctypes.c_int
+    if L.epik2_probe_tc_fp4(device, ctypes.byref(m)) == 0:
+        out["tc_fp4_mac_per_s"] = m.value
     return out
 
 

@@ -1,5 +1,5 @@
 /*
- * epik2_probe.h -- measured integer-pipe peaks of a device (libepik2_probe.so).
+ * epik2_probe.h -- measured integer-pipe and tensor-core peaks of a device (libepik2_probe.so).
  *
  * No reference counterpart.  The roofline of the integer search kernel is the POPC
  * issue rate, which no vendor table gives for this GPU; these probes measure it (and
@@ -20,6 +20,11 @@ int epik2_probe_int_peaks(int device, double *popc_per_s, double *lop3_per_s, do
  * accumulators in tensor memory); result in multiply-accumulates per second.  Waits are
  * bounded; returns -6 if one expired. */
 int epik2_probe_tc_i8(int device, double *mac_per_s);
+
+/* Dense block-scaled FP4 tensor-core rate in the search kernel's FP4 shape: back-to-back
+ * tcgen05.mma kind::mxf4 (M=128, N=224, K=64, E2M1 operands, UE8M0 scale factors in tensor
+ * memory, FP32 accumulators); multiply-accumulates per second.  Same waits and errors. */
+int epik2_probe_tc_fp4(int device, double *mac_per_s);
 
 #ifdef __cplusplus
 }

@@ -29,7 +29,7 @@ def test_probe_library_exports_every_declared_symbol():
     import ctypes as C
     lib = C.CDLL(epik2.PROBE_LIB_PATH)
     declared = epik2.exported_symbols(epik2.PROBE_HEADER)
-    assert declared == ["epik2_probe_int_peaks", "epik2_probe_tc_i8"]
+    assert declared == ["epik2_probe_int_peaks", "epik2_probe_tc_fp4", "epik2_probe_tc_i8"]
     assert all(hasattr(lib, s) for s in declared)
 
 
