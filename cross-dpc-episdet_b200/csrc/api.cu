@@ -34,6 +34,8 @@ struct epik2_ctx {
   int64_t* d_pb_off = nullptr;
   uint32_t* d_pb_ij = nullptr;
   int64_t pb_cap = 0;
+  uint64_t* d_tiles = nullptr;  // tensor-core tile descriptors
+  int64_t tiles_cap = 0;
   unsigned long long* d_counter = nullptr;
   BestSlot* d_slots = nullptr;  // one per warp of the scan grid
   BestSlot* d_best = nullptr;
@@ -55,11 +57,13 @@ struct epik2_ctx {
 constexpr size_t kMaxPlans = 32;  // cached batched plans per context
 
 struct BatchPlan {
-  int kw = 4;
   int64_t n_tiles = 0;
+  std::vector<int> group_code;           // stage_words * 2 + FP4 of each launch group
+  std::vector<int64_t> group_off;        // tiles of group g: [group_off[g], group_off[g+1])
+  unsigned long long* d_counters = nullptr;  // one tile counter per group
   int32_t n_jobs = 0;
   epik2::TcJob* d_jobs = nullptr;
-  int64_t* d_job_off = nullptr;
+  uint64_t* d_tiles = nullptr;           // descriptors of every job's tiles, job after job
   int64_t* d_pb_off = nullptr;
   uint32_t* d_pb_ij = nullptr;
   epik2::BestSlot* d_job_slots = nullptr;
@@ -69,8 +73,6 @@ struct BatchPlan {
   epik2::Rescored* h_resc = nullptr;     // pinned
   int* h_err = nullptr;                  // pinned
   std::vector<epik2::TcJob> h_jobs;
-  std::vector<int64_t> pb_base;          // offset of each job's pair-block tile prefix sums
-  std::vector<int64_t> pb_ij_base;       // offset of each job's (i, j0) list
   bool rescore = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -78,7 +80,8 @@ struct BatchPlan {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     cudaFree(d_jobs);
-    cudaFree(d_job_off);
+    cudaFree(d_tiles);
+    cudaFree(d_counters);
     cudaFree(d_pb_off);
     cudaFree(d_pb_ij);
     cudaFree(d_job_slots);
@@ -187,6 +190,16 @@ int ensure_pb(epik2_ctx* ctx, int64_t n) {
   CK(ctx, cudaMalloc(&ctx->d_pb_off, (size_t)(n + 1) * 8), "alloc tile list");
   CK(ctx, cudaMalloc(&ctx->d_pb_ij, (size_t)n * 8), "alloc tile list");
   ctx->pb_cap = n;
+  return EPIK2_OK;
+}
+
+int ensure_tiles(epik2_ctx* ctx, int64_t n) {
+  if (n <= ctx->tiles_cap) return EPIK2_OK;
+  cudaFree(ctx->d_tiles);
+  ctx->d_tiles = nullptr;
+  ctx->tiles_cap = 0;
+  CK(ctx, cudaMalloc(&ctx->d_tiles, (size_t)n * 8), "alloc tile descriptors");
+  ctx->tiles_cap = n;
   return EPIK2_OK;
 }
 
@@ -377,12 +390,17 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   const int64_t n_pb = (int64_t)off.size() - 1;
   int r = ensure_pb(ctx, std::max<int64_t>(n_pb, 1));
   if (r) return r;
+  r = ensure_tiles(ctx, std::max<int64_t>(off.back(), 1));
+  if (r) return r;
   if (n_pb > 0) {
     CK(ctx, cudaMemcpyAsync(ctx->d_pb_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, ctx->stream),
        "upload tile list");
     CK(ctx, cudaMemcpyAsync(ctx->d_pb_ij, ij.data(), ij.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
        "upload tile list");
     ctx->stats.h2d_bytes += off.size() * 8 + ij.size() * 4;
+    CK(ctx, launch_expand_tiles(ctx->d_pb_off, ctx->d_pb_ij, n_pb, fp4, 0, ctx->d_tiles, ctx->stream),
+       "tile descriptors");
+    ctx->stats.kernel_launches += 1;
   }
   CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream), "reset counter");
   CK(ctx, cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream), "reset error word");
@@ -391,9 +409,7 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   p.singles = d.singles;
   p.pairs = d.pairs;
   p.lut = d.lut;
-  p.pb_off = ctx->d_pb_off;
-  p.pb_ij = ctx->d_pb_ij;
-  p.n_pb = std::max<int64_t>(n_pb, 1);
+  p.tiles = ctx->d_tiles;
   p.n_tiles = off.back();
   p.tri = d.tri;
   p.m = (int32_t)m;
@@ -505,12 +521,17 @@ int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
 }
 
 // Batched form: build (or reuse) the plan for these datasets, refresh the job table from
-// the datasets' current class split, replay the captured launch sequence.
-int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vector<int32_t>& ids, int kw,
-              bool fp4, bool rescore, epik2_best* out) {
+// the datasets' current class split, replay the captured launch sequence.  codes[b] =
+// stage_words * 2 + (FP4 ? 1 : 0) of dataset b; datasets with the same code form a group,
+// one persistent tensor-core launch per group (inside the one graph), each group with its
+// own tile queue (datasets with the most samples first).
+int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vector<int32_t>& ids,
+              const std::vector<int>& codes, bool rescore, epik2_best* out) {
+  (void)ids;
   std::vector<int64_t> key;
   for (const DevDataset* d : ds) key.push_back(d->n_snps);
-  key.push_back(kw * 4 + (fp4 ? 2 : 0) + (rescore ? 1 : 0));
+  for (int c : codes) key.push_back(c);
+  key.push_back(rescore ? 1 : 0);
   BatchPlan* plan = nullptr;
   auto it = ctx->plans.find(key);
   const int32_t n = (int32_t)ds.size();
@@ -530,19 +551,32 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
       ctx->plan_lru.erase(ctx->plan_lru.begin());
     }
     std::unique_ptr<BatchPlan> pl(new BatchPlan());
-    pl->kw = kw;
     pl->n_jobs = n;
     pl->rescore = rescore;
-    // pair-block lists depend on the SNP count only: one list per distinct count
-    std::vector<int64_t> job_off(1, 0), pb_off_all;
+    // groups in order of first appearance
+    std::vector<int> group_code;
+    std::vector<int> group_of(n);
+    for (int32_t b = 0; b < n; b++) {
+      auto g = std::find(group_code.begin(), group_code.end(), codes[b]);
+      if (g == group_code.end()) {
+        group_code.push_back(codes[b]);
+        g = group_code.end() - 1;
+      }
+      group_of[b] = (int)(g - group_code.begin());
+    }
+    const int n_groups = (int)group_code.size();
+    // pair-block lists depend on the SNP count and the k-block size: one list per pair
+    std::vector<int64_t> pb_off_all;
     std::vector<uint32_t> pb_ij_all;
+    std::vector<int64_t> job_pb_base(n), job_ij_base(n), job_n_pb(n), job_tiles(n);
     struct ListInfo {
       int64_t off_base, ij_base, n_pb, tiles;
     };
-    std::map<int64_t, ListInfo> lists;
+    std::map<std::pair<int64_t, int64_t>, ListInfo> lists;
     for (int32_t b = 0; b < n; b++) {
+      const bool fp4 = codes[b] & 1;
       const int64_t m = ds[b]->n_snps, kk = tc_k_per_tile(fp4), n_kb = (m + kk - 1) / kk;
-      auto li = lists.find(m);
+      auto li = lists.find({m, kk});
       if (li == lists.end()) {
         ListInfo L{(int64_t)pb_off_all.size(), (int64_t)pb_ij_all.size(), 0, 0};
         pb_off_all.push_back(0);
@@ -554,26 +588,42 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
             pb_off_all.push_back(L.tiles);
             L.n_pb++;
           }
-        li = lists.emplace(m, L).first;
+        li = lists.emplace(std::make_pair(m, kk), L).first;
       }
-      pl->pb_base.push_back(li->second.off_base);
-      pl->pb_ij_base.push_back(li->second.ij_base);
-      job_off.push_back(job_off.back() + li->second.tiles);
-      TcJob j{};
-      j.n_pb = std::max<int64_t>(li->second.n_pb, 1);
-      pl->h_jobs.push_back(j);
+      job_pb_base[b] = li->second.off_base;
+      job_ij_base[b] = li->second.ij_base;
+      job_n_pb[b] = li->second.n_pb;
+      job_tiles[b] = li->second.tiles;
+      pl->h_jobs.push_back(TcJob{});
     }
-    pl->n_tiles = job_off.back();
+    // tile queue: group after group; inside a group, datasets with the most samples first
+    // (their tiles are the longest), so the short tiles fill the end of each launch
+    std::vector<int32_t> order(n);
+    for (int32_t b = 0; b < n; b++) order[b] = b;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+      if (group_of[a] != group_of[b]) return group_of[a] < group_of[b];
+      return ds[a]->n_samples > ds[b]->n_samples;
+    });
+    std::vector<int64_t> job_off(n, 0);
+    pl->group_off.assign(n_groups + 1, 0);
+    pl->n_tiles = 0;
+    for (int32_t b : order) {
+      job_off[b] = pl->n_tiles;
+      pl->n_tiles += job_tiles[b];
+      pl->group_off[group_of[b] + 1] = pl->n_tiles;
+    }
+    for (int g = 1; g <= n_groups; g++) pl->group_off[g] = std::max(pl->group_off[g], pl->group_off[g - 1]);
+    pl->group_code = group_code;
     const size_t pb_ij_bytes = std::max<size_t>(pb_ij_all.size(), 2) * 4;
-    if (cudaMalloc(&pl->d_jobs, sizeof(TcJob) * n) || cudaMalloc(&pl->d_job_off, 8 * (n + 1)) ||
+    if (cudaMalloc(&pl->d_jobs, sizeof(TcJob) * n) ||
+        cudaMalloc(&pl->d_tiles, 8 * (size_t)std::max<int64_t>(pl->n_tiles, 1)) ||
+        cudaMalloc(&pl->d_counters, 8 * (size_t)n_groups) ||
         cudaMalloc(&pl->d_pb_off, 8 * pb_off_all.size()) || cudaMalloc(&pl->d_pb_ij, pb_ij_bytes) ||
         cudaMalloc(&pl->d_job_slots, sizeof(BestSlot) * (size_t)n * grid) ||
         cudaMalloc(&pl->d_results, sizeof(BestSlot) * n) || cudaMallocHost(&pl->h_results, sizeof(BestSlot) * n) ||
         cudaMallocHost(&pl->h_err, sizeof(int)) || cudaMalloc(&pl->d_resc, sizeof(Rescored) * n) ||
         cudaMallocHost(&pl->h_resc, sizeof(Rescored) * n))
       return fail(ctx, EPIK2_E_NOMEM, "batched plan: device memory");
-    CK(ctx, cudaMemcpyAsync(pl->d_job_off, job_off.data(), 8 * (n + 1), cudaMemcpyHostToDevice, ctx->stream),
-       "upload batch");
     CK(ctx, cudaMemcpyAsync(pl->d_pb_off, pb_off_all.data(), 8 * pb_off_all.size(), cudaMemcpyHostToDevice,
                             ctx->stream),
        "upload batch");
@@ -581,26 +631,36 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
       CK(ctx, cudaMemcpyAsync(pl->d_pb_ij, pb_ij_all.data(), 4 * pb_ij_all.size(), cudaMemcpyHostToDevice,
                               ctx->stream),
          "upload batch");
-    ctx->stats.h2d_bytes += 8 * (n + 1) + 8 * pb_off_all.size() + 4 * pb_ij_all.size();
+    ctx->stats.h2d_bytes += 8 * pb_off_all.size() + 4 * pb_ij_all.size();
+    for (int32_t b = 0; b < n; b++) {
+      CK(ctx, launch_expand_tiles(pl->d_pb_off + job_pb_base[b], pl->d_pb_ij + job_ij_base[b], job_n_pb[b],
+                                  codes[b] & 1, b, pl->d_tiles + job_off[b], ctx->stream),
+         "tile descriptors");
+      ctx->stats.kernel_launches += 1;
+    }
     CK(ctx, cudaStreamSynchronize(ctx->stream), "upload batch");
-    // capture: reset slots, counter and error word; batched search; per-dataset reduce; read back
-    TcParams p{};
-    p.counter = ctx->d_counter;
-    p.err = ctx->d_err;
-    p.jobs = pl->d_jobs;
-    p.job_tile_off = pl->d_job_off;
-    p.n_jobs = n;
-    p.job_slots = pl->d_job_slots;
-    p.n_tiles = pl->n_tiles;
-    p.n_pb = 1;
+    // capture: reset slots, counters and error word; one batched search per group;
+    // per-dataset reduce; optional FP64 rescore; read back
     CK(ctx, tc_configure(), "configure");
     CK(ctx, launch_fill_slots(pl->d_job_slots, (int64_t)n * grid, ctx->stream), "configure");  // also loads modules
     CK(ctx, cudaStreamSynchronize(ctx->stream), "configure");
     CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
     cudaError_t e = launch_fill_slots(pl->d_job_slots, (int64_t)n * grid, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pl->d_counters, 0, 8 * (size_t)n_groups, ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream);
-    if (e == cudaSuccess) e = launch_scan_tc(p, grid, kw, fp4, false, ctx->stream);
+    for (int g = 0; g < n_groups && e == cudaSuccess; g++) {
+      const int64_t nt = pl->group_off[g + 1] - pl->group_off[g];
+      if (nt == 0) continue;
+      TcParams p{};
+      p.counter = pl->d_counters + g;
+      p.err = ctx->d_err;
+      p.jobs = pl->d_jobs;
+      p.tiles = pl->d_tiles + pl->group_off[g];
+      p.n_jobs = n;
+      p.job_slots = pl->d_job_slots;
+      p.n_tiles = nt;
+      e = launch_scan_tc(p, grid, group_code[g] >> 1, group_code[g] & 1, false, ctx->stream);
+    }
     if (e == cudaSuccess) e = launch_reduce_jobs(pl->d_job_slots, n, grid, pl->d_results, ctx->stream);
     if (e == cudaSuccess && rescore) e = launch_rescore_jobs(pl->d_jobs, pl->d_results, n, pl->d_resc, ctx->stream);
     if (e == cudaSuccess && rescore)
@@ -624,8 +684,6 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     j.singles = d.singles;
     j.pairs = d.pairs;
     j.lut = d.lut;
-    j.pb_off = plan->d_pb_off + plan->pb_base[b];
-    j.pb_ij = plan->d_pb_ij + plan->pb_ij_base[b];
     j.lut64 = d.lut64;
     j.tri = d.tri;
     j.m = (int32_t)d.n_snps;
@@ -642,7 +700,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
   CK(ctx, cudaGraphLaunch(plan->exec, ctx->stream), "batched graph launch");
   CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
   CK(ctx, cudaStreamSynchronize(ctx->stream), "batched search");
-  ctx->stats.kernel_launches += 3;
+  ctx->stats.kernel_launches += 2 + (uint64_t)plan->group_code.size() + (rescore ? 1 : 0);
   ctx->stats.d2h_bytes += sizeof(BestSlot) * n + 4;
   if (*plan->h_err) return fail(ctx, EPIK2_E_TIMEOUT, "batched search: a bounded wait expired");
   float kms = 0.0f;
@@ -731,6 +789,7 @@ void epik2_destroy(epik2_ctx* ctx) {
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_pb_off);
   cudaFree(ctx->d_pb_ij);
+  cudaFree(ctx->d_tiles);
   cudaFreeHost(ctx->h_best);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
@@ -1021,47 +1080,50 @@ int epik2_autotune(epik2_ctx* ctx, int32_t dataset_id, epik2_tune* out) {
 int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, const epik2_opts* opts, epik2_best* out) {
   if (!ctx) return EPIK2_E_INVALID;
   if (!dataset_ids || !out || n < 1) return fail(ctx, EPIK2_E_INVALID, "bad dataset list");
+  if (n > kMaxBatchJobs) return fail(ctx, EPIK2_E_TOO_LARGE, "at most 512 datasets per batched launch");
   std::vector<DevDataset*> ds;
   std::vector<int32_t> ids(dataset_ids, dataset_ids + n);
-  DevDataset* largest = nullptr;
   for (int32_t b = 0; b < n; b++) {
     DevDataset* d = find(ctx, dataset_ids[b]);
     if (!d) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset in batch");
     if (d->n_snps < 3) return fail(ctx, EPIK2_E_INVALID, "every dataset needs at least 3 SNPs");
     ds.push_back(d);
-    const double w = (double)triplets_before(d->n_snps, d->n_snps) * (double)d->n_samples;
-    if (!largest || w > (double)triplets_before(largest->n_snps, largest->n_snps) * (double)largest->n_samples)
-      largest = d;
   }
   CK(ctx, cudaSetDevice(ctx->device), "set device");
-  // format: the requested tensor-core format, else the autotuner's choice for the largest
-  // dataset (int8 when it chose the integer engine or when a class is too large for FP4)
-  bool all_fp4 = true;
-  for (const DevDataset* d : ds) all_fp4 = all_fp4 && fp4_exact(*d);
-  int engine = opts ? opts->engine : 0;
-  if (engine == EPIK2_ENGINE_INT) return fail(ctx, EPIK2_E_INVALID, "the batched form runs on the tensor cores");
-  if (engine < 0 || engine > EPIK2_ENGINE_TC_FP4) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
-  if (engine == EPIK2_ENGINE_TC_FP4 && !all_fp4)
-    return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
-  int kw = (opts && opts->stage_words) ? opts->stage_words : 0;
-  if (engine == 0 || kw == 0) {
-    epik2_tune t{};
-    int r = tuned(ctx, *largest, &t);
-    if (r) return r;
-    if (engine == 0) {  // a requested stage depth that only one format takes picks that format
-      engine = (t.engine == EPIK2_ENGINE_TC_FP4 && all_fp4) ? EPIK2_ENGINE_TC_FP4 : EPIK2_ENGINE_TC;
-      if (kw == 4) engine = EPIK2_ENGINE_TC;
-      if (kw == 16 && all_fp4) engine = EPIK2_ENGINE_TC_FP4;
+  // format and stage depth per dataset: the requested ones, else the autotuner's choice
+  // for the dataset's shape (int8 when it chose the integer engine, or when a class is too
+  // large for FP4 accumulators).  Datasets with the same choice share one launch.
+  const int engine_req = opts ? opts->engine : 0;
+  const int kw_req = opts ? opts->stage_words : 0;
+  if (engine_req == EPIK2_ENGINE_INT) return fail(ctx, EPIK2_E_INVALID, "the batched form runs on the tensor cores");
+  if (engine_req < 0 || engine_req > EPIK2_ENGINE_TC_FP4) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
+  std::vector<int> codes;  // stage_words * 2 + (FP4 ? 1 : 0) per dataset
+  for (DevDataset* d : ds) {
+    const bool can_fp4 = fp4_exact(*d);
+    if (engine_req == EPIK2_ENGINE_TC_FP4 && !can_fp4)
+      return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
+    int engine = engine_req, kw = kw_req;
+    if (engine == 0 || kw == 0) {
+      epik2_tune t{};
+      int r = tuned(ctx, *d, &t);
+      if (r) return r;
+      if (engine == 0) {  // a requested stage depth that only one format takes picks that format
+        engine = (t.engine == EPIK2_ENGINE_TC_FP4 && can_fp4) ? EPIK2_ENGINE_TC_FP4 : EPIK2_ENGINE_TC;
+        if (kw == 4) engine = EPIK2_ENGINE_TC;
+        if (kw == 16 && can_fp4) engine = EPIK2_ENGINE_TC_FP4;
+      }
+      if (kw == 0) {
+        if (engine == EPIK2_ENGINE_TC_FP4) kw = t.rate_fp4_16 > t.rate_fp4_8 ? 16 : 8;
+        else kw = t.rate_tc8 >= t.rate_tc4 ? 8 : 4;
+      }
     }
-    if (kw == 0) {
-      if (engine == EPIK2_ENGINE_TC_FP4) kw = t.rate_fp4_16 > t.rate_fp4_8 ? 16 : 8;
-      else kw = t.rate_tc8 >= t.rate_tc4 ? 8 : 4;
-    }
+    const bool fp4 = engine == EPIK2_ENGINE_TC_FP4;
+    if (!fp4 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
+    if (fp4 && kw != 8 && kw != 16)
+      return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 8 or 16 with the FP4 engine");
+    codes.push_back(kw * 2 + (fp4 ? 1 : 0));
   }
-  const bool fp4 = engine == EPIK2_ENGINE_TC_FP4;
-  if (!fp4 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
-  if (fp4 && kw != 8 && kw != 16) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 8 or 16 with the FP4 engine");
-  return run_batch(ctx, ds, ids, kw, fp4, opts && opts->rescore_fp64, out);
+  return run_batch(ctx, ds, ids, codes, opts && opts->rescore_fp64, out);
 }
 
 int epik2_dump_tables(epik2_ctx* ctx, int32_t dataset_id, uint32_t* tables, float* scores) {

@@ -83,23 +83,30 @@ struct TcJob {
   const uint4* pairs;
   const float* lut;
   const double* lut64;
-  const int64_t* pb_off;
-  const uint32_t* pb_ij;
-  int64_t n_pb;
   int64_t tri;
   int32_t m, m_pad, w0, w1, n0, n1;
 };
 
+// Tensor-core tile descriptor: first index i (bits 0-19), first SNP j0 of the pair block
+// (bits 20-39), k block (bits 40-53: k in [kK*kb, kK*kb + kK)), batched job (bits 54-62).
+__host__ __device__ inline uint64_t pack_tile(uint32_t i, uint32_t j0, uint32_t kb, uint32_t job) {
+  return (uint64_t)i | ((uint64_t)j0 << 20) | ((uint64_t)kb << 40) | ((uint64_t)job << 54);
+}
+__host__ __device__ inline int tile_i(uint64_t d) { return (int)(d & 0xFFFFF); }
+__host__ __device__ inline int tile_j0(uint64_t d) { return (int)((d >> 20) & 0xFFFFF); }
+__host__ __device__ inline int tile_kb(uint64_t d) { return (int)((d >> 40) & 0x3FFF); }
+__host__ __device__ inline int tile_job(uint64_t d) { return (int)((d >> 54) & 0x1FF); }
+constexpr int kMaxBatchJobs = 512;  // datasets per batched launch (9 descriptor bits)
+
 // Tensor-core engine parameters (scan_tc.cu).  Tiles: for each pair block (i, j0..j0+31)
-// the k blocks [128*kb, 128*kb+128) with kb from (j0+1)/128 to ceil(m/128)-1.
+// the k blocks [kK*kb, kK*kb+kK) with kb from (j0+1)/kK to ceil(m/kK)-1 (kK = 128 int8,
+// 112 FP4), one descriptor (pack_tile) per tile, taken in order from a shared counter.
 struct TcParams {
   const uint2* planes;
   const uint32_t* singles;
   const uint4* pairs;
   const float* lut;
-  const int64_t* pb_off;   // prefix sums of tiles per pair block, [n_pb + 1]
-  const uint32_t* pb_ij;   // (i, j0) per pair block
-  int64_t n_pb;
+  const uint64_t* tiles;   // [n_tiles] descriptors
   int64_t n_tiles;
   int64_t tri;
   int32_t m, m_pad, w0, w1, n0, n1;
@@ -110,9 +117,8 @@ struct TcParams {
   uint32_t* dump_tables;
   float* dump_scores;
   int* err;                // set to 1 if a bounded wait expired
-  // batched form (jobs != null): tiles of job b are [job_tile_off[b], job_tile_off[b+1])
+  // batched form (jobs != null): each tile's descriptor names its job
   const TcJob* jobs;
-  const int64_t* job_tile_off;
   int32_t n_jobs;
   BestSlot* job_slots;     // [n_jobs][grid]
 };
@@ -129,6 +135,10 @@ int scan_blocks_per_sm();
 cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool dump,
                            cudaStream_t stream);
 int tc_k_per_tile(bool fp4);  // SNPs k per tensor-core tile: 128 (int8) or 112 (FP4)
+// Tile descriptors of one pair-block list (prefix sums pb_off[0..n_pb], (i, j0) pairs) into
+// out[pb_off[b] ...], tagged with `job`.
+cudaError_t launch_expand_tiles(const int64_t* pb_off, const uint32_t* pb_ij, int64_t n_pb, bool fp4, int job,
+                                uint64_t* out, cudaStream_t stream);
 cudaError_t launch_reduce_jobs(const BestSlot* slots, int n_jobs, int per_job, BestSlot* out, cudaStream_t stream);
 cudaError_t launch_fill_slots(BestSlot* slots, int64_t n, cudaStream_t stream);
 cudaError_t tc_configure();

@@ -181,9 +181,7 @@ struct JobView {
   const uint32_t* singles;
   const uint4* pairs;
   const float* lut;
-  const int64_t* pb_off;
-  const uint32_t* pb_ij;
-  int64_t n_pb, tri;
+  int64_t tri;
   int32_t m, m_pad, w0, w1, n0, n1;
 };
 
@@ -254,40 +252,73 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   uint32_t g_chunk = 0, n_tile = 0;
   const uint32_t* E = reinterpret_cast<const uint32_t*>(smem);  // epilogue staging, reuses the stages
 
-  for (;;) {
-    if (tid == 0) s_tile = (long long)atomicAdd(p.counter, 1ull);
-    __syncthreads();
-    long long tile = s_tile;
-    if (tile >= p.n_tiles || s_abort) break;
-    JobView jv;
-    int job = 0;
-    if (kBatched) {
-      int lo = 0, hi = p.n_jobs;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (p.job_tile_off[mid] <= tile) lo = mid;
-        else hi = mid;
+  // Batched form: fold the CTA's candidates for dataset jb into its slot of that dataset.
+  // Called by every thread when the dataset of the next tile differs (the queue holds each
+  // dataset's tiles together, so this happens about once per dataset and CTA).
+  auto flush_job = [&](int jb) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const float os = __shfl_xor_sync(kFull, best_s, off);
+      const unsigned long long ok = __shfl_xor_sync(kFull, best_k, off);
+      if (better(os, ok, best_s, best_k)) {
+        best_s = os;
+        best_k = ok;
       }
-      job = lo;
-      tile -= p.job_tile_off[job];
+    }
+    if (lane == 0 && worker) {
+      s_red_s[warp] = best_s;
+      s_red_k[warp] = best_k;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      float bs = s_red_s[0];
+      unsigned long long bk = s_red_k[0];
+      for (int w = 1; w < kTcWarps; w++)
+        if (better(s_red_s[w], s_red_k[w], bs, bk)) {
+          bs = s_red_s[w];
+          bk = s_red_k[w];
+        }
+      BestSlot& slot = p.job_slots[(int64_t)jb * gridDim.x + blockIdx.x];
+      if (better(bs, bk, slot.score, slot.key)) {
+        slot.score = bs;
+        slot.key = bk;
+      }
+    }
+    __syncthreads();
+    best_s = FLT_MAX;
+    best_k = ~0ull;
+  };
+  int cur_job = -1;
+
+  for (;;) {
+    // next tile from the shared queue; its descriptor (one 8-byte load) gives the dataset,
+    // the first index, the pair block and the k block
+    if (tid == 0) {
+      const unsigned long long t = atomicAdd(p.counter, 1ull);
+      s_tile = (t < (unsigned long long)p.n_tiles && !s_abort) ? (long long)__ldg(p.tiles + t) : -1ll;
+    }
+    __syncthreads();
+    const long long desc = s_tile;
+    if (kBatched) {  // desc is the same for every thread: the flush is uniform
+      const int next_job = desc < 0 ? -1 : tile_job(desc);
+      if (next_job != cur_job) {
+        if (cur_job >= 0) flush_job(cur_job);
+        cur_job = next_job;
+      }
+    }
+    if (desc < 0) break;
+    const int i = tile_i(desc), j0 = tile_j0(desc), k0 = kK * tile_kb(desc);
+    const int job = kBatched ? tile_job(desc) : 0;
+    JobView jv;
+    if (kBatched) {
       const TcJob& J = p.jobs[job];
-      jv = JobView{J.planes, J.singles, J.pairs, J.lut, J.pb_off, J.pb_ij, J.n_pb, J.tri,
-                   J.m, J.m_pad, J.w0, J.w1, J.n0, J.n1};
+      jv = JobView{J.planes, J.singles, J.pairs, J.lut, J.tri, J.m, J.m_pad, J.w0, J.w1, J.n0, J.n1};
     } else {
-      jv = JobView{p.planes, p.singles, p.pairs, p.lut, p.pb_off, p.pb_ij, p.n_pb, p.tri,
-                   p.m, p.m_pad, p.w0, p.w1, p.n0, p.n1};
+      jv = JobView{p.planes, p.singles, p.pairs, p.lut, p.tri, p.m, p.m_pad, p.w0, p.w1, p.n0, p.n1};
     }
     const int64_t m_pad = jv.m_pad;
     const int m = jv.m;
     const int nc0 = (jv.w0 + kW - 1) / kW, nc1 = (jv.w1 + kW - 1) / kW, nct = nc0 + nc1;
-    int64_t lo = 0, hi = jv.n_pb;
-    while (hi - lo > 1) {
-      const int64_t mid = (lo + hi) >> 1;
-      if (jv.pb_off[mid] <= tile) lo = mid;
-      else hi = mid;
-    }
-    const int i = (int)jv.pb_ij[2 * lo], j0 = (int)jv.pb_ij[2 * lo + 1];
-    const int k0 = kK * ((j0 + 1) / kK + (int)(tile - jv.pb_off[lo]));
 
     // ---- operand expansion and MMA, 32*kW samples per stage ----
     // Units of a stage, kU of each kind per thread (r < kU):
@@ -514,39 +545,6 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       }
       __syncthreads();  // the staging buffer is rewritten by the next half / next tile
     }
-    if (kBatched) {
-      // fold the tile's candidates into this CTA's slot of the tile's dataset
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const float os = __shfl_xor_sync(kFull, best_s, off);
-        const unsigned long long ok = __shfl_xor_sync(kFull, best_k, off);
-        if (better(os, ok, best_s, best_k)) {
-          best_s = os;
-          best_k = ok;
-        }
-      }
-      if (lane == 0 && worker) {
-        s_red_s[warp] = best_s;
-        s_red_k[warp] = best_k;
-      }
-      __syncthreads();
-      if (tid == 0) {
-        float bs = s_red_s[0];
-        unsigned long long bk = s_red_k[0];
-        for (int w = 1; w < kTcWarps; w++)
-          if (better(s_red_s[w], s_red_k[w], bs, bk)) {
-            bs = s_red_s[w];
-            bk = s_red_k[w];
-          }
-        BestSlot& slot = p.job_slots[(int64_t)job * gridDim.x + blockIdx.x];
-        if (better(bs, bk, slot.score, slot.key)) {
-          slot.score = bs;
-          slot.key = bk;
-        }
-      }
-      best_s = FLT_MAX;
-      best_k = ~0ull;
-    }
   }
 
   // ---- teardown: every MMA has completed (its tile's accumulator barrier was waited) ----
@@ -577,6 +575,27 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       p.cand[gwarp * 32 + lane].key = list_k;
     }
   }
+}
+
+// Tile descriptors of one pair-block list: pair block b = (i, j0) holds the tiles
+// [pb_off[b], pb_off[b+1]) with k blocks (j0+1)/kK, (j0+1)/kK + 1, ...; one thread per
+// pair block writes them to out[pb_off[b] ...].
+__global__ void k_expand_tiles(const int64_t* __restrict__ pb_off, const uint32_t* __restrict__ pb_ij, int64_t n_pb,
+                               int kK, int job, uint64_t* __restrict__ out) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n_pb) return;
+  const uint32_t i = pb_ij[2 * b], j0 = pb_ij[2 * b + 1];
+  const uint32_t kb0 = (j0 + 1) / (uint32_t)kK;
+  const int64_t t0 = pb_off[b], n = pb_off[b + 1] - t0;
+  for (int64_t t = 0; t < n; t++) out[t0 + t] = pack_tile(i, j0, kb0 + (uint32_t)t, (uint32_t)job);
+}
+
+cudaError_t launch_expand_tiles(const int64_t* pb_off, const uint32_t* pb_ij, int64_t n_pb, bool fp4, int job,
+                                uint64_t* out, cudaStream_t stream) {
+  if (n_pb <= 0) return cudaSuccess;
+  k_expand_tiles<<<(unsigned)((n_pb + 255) / 256), 256, 0, stream>>>(pb_off, pb_ij, n_pb, tc_k_per_tile(fp4), job,
+                                                                     out);
+  return cudaGetLastError();
 }
 
 // Per-dataset reduction of the batched search's per-CTA slots: block b reduces dataset b.

@@ -92,7 +92,7 @@ struct epik2_server {
 
   void run() {
     const double target = opts.batch_work > 0 ? opts.batch_work : 2e13;
-    const int32_t max_active = opts.max_active > 0 ? opts.max_active : 256;
+    const int32_t max_active = std::min(opts.max_active > 0 ? opts.max_active : 256, 512);  // one batched launch
     const int64_t reserve = opts.hbm_reserve_bytes > 0 ? opts.hbm_reserve_bytes : (int64_t)2 << 30;
     for (;;) {
       std::vector<Item> batch;

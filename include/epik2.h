@@ -180,7 +180,8 @@ int epik2_scan_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int
  * out[0..n).  The launch sequence is captured once per set of datasets into a CUDA
  * graph and replayed (phenotype re-encodings via epik2_set_pheno are picked up).  The
  * stage depth is opts->stage_words or, when 0, the autotuner's choice for the largest
- * dataset.  Each result equals epik2_scan on that dataset alone.
+ * dataset.  Each result equals epik2_scan on that dataset alone.  At most 512 datasets per
+ * call (EPIK2_E_TOO_LARGE beyond).
  * ------------------------------------------------------------------------------ */
 int epik2_scan_batch(epik2_ctx *ctx, const int32_t *dataset_ids, int32_t n, const epik2_opts *opts,
                      epik2_best *out);

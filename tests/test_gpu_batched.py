@@ -92,3 +92,18 @@ def test_fp4_refuses_classes_of_2_24_samples():
         b8 = ctx.scan(d, engine=epik2.ENGINE_TC)
         bi = ctx.scan(d, engine=epik2.ENGINE_INT)
     assert b8.ijk == bi.ijk == (0, 1, 2) and f32_bits(b8.score) == f32_bits(bi.score)
+
+
+def test_batch_limit_and_tiny_datasets():
+    """512 datasets fit one batched launch (the tile descriptors name the dataset in 9
+    bits); 513 are refused.  Tiny datasets (3..5 SNPs) still match the oracle."""
+    data = [O.gen_hwe(2000 + t, 64, 3 + t % 3, 32) for t in range(513)]
+    with epik2.Context(0) as ctx:
+        ids = [ctx.load(g, p) for g, p in data]
+        got = ctx.scan_batch(ids[:512])
+        with pytest.raises(epik2.Epik2Error) as e:
+            ctx.scan_batch(ids)
+        assert e.value.status == epik2.E_TOO_LARGE
+    for (g, p), b in list(zip(data, got))[::37]:
+        r = O.scan(g, p)
+        assert b.ijk == r["ijk"] and f32_bits(b.score) == f32_bits(r["score"])
