@@ -180,8 +180,11 @@ void decode_key(unsigned long long key, uint32_t& i, uint32_t& j, uint32_t& k) {
   k = (uint32_t)(key & ((1ull << 21) - 1));
 }
 
+// Scratch buffers grow geometrically: a reallocation (which synchronises the device) happens
+// O(log n) times, not whenever a slightly larger search comes.
 int ensure_pb(epik2_ctx* ctx, int64_t n) {
   if (n <= ctx->pb_cap) return EPIK2_OK;
+  n = std::max(n, 2 * ctx->pb_cap);
   cudaFree(ctx->d_pb_off);
   cudaFree(ctx->d_pb_ij);
   ctx->d_pb_off = nullptr;
@@ -195,6 +198,7 @@ int ensure_pb(epik2_ctx* ctx, int64_t n) {
 
 int ensure_tiles(epik2_ctx* ctx, int64_t n) {
   if (n <= ctx->tiles_cap) return EPIK2_OK;
+  n = std::max(n, 2 * ctx->tiles_cap);
   cudaFree(ctx->d_tiles);
   ctx->d_tiles = nullptr;
   ctx->tiles_cap = 0;
@@ -205,6 +209,7 @@ int ensure_tiles(epik2_ctx* ctx, int64_t n) {
 
 int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
   if (n <= ctx->pgoff_cap) return EPIK2_OK;
+  n = std::max(n, 2 * ctx->pgoff_cap);
   if (ctx->d_pgoff) cudaFree(ctx->d_pgoff);
   ctx->d_pgoff = nullptr;
   ctx->pgoff_cap = 0;

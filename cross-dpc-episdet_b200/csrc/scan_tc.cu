@@ -321,45 +321,47 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     const int nc0 = (jv.w0 + kW - 1) / kW, nc1 = (jv.w1 + kW - 1) / kW, nct = nc0 + nc1;
 
     // ---- operand expansion and MMA, 32*kW samples per stage ----
-    // Units of a stage, kU of each kind per thread (r < kU):
-    //   A: word w = (tid>>7) + 4r, row = tid&127 = 32*ab + q (pair q, g_i = ab>>1, g_j = ab&1)
-    //   B: word w = (tid>>7) + 4r, kl = tid&127 (< kK) -> rows kK*c + kl (g_k = c) of both c
+    // Work of a stage per thread:
+    //   A: pair q = lane, word wA = warp % kW: loads the i and j words once and writes rows
+    //      32*ab + q (g_i = ab>>1, g_j = ab&1) for kAb = kW/4 consecutive ab
+    //   B: words w = (tid>>7) + 4r (r < kU), kl = tid&127 (< kK) -> rows kK*c + kl (g_k = c)
+    //      of both c
     // A warp writes 32 consecutive rows of one 16-byte K group per store (conflict-free).
     // The words of stage cc+1 are loaded while stage cc is expanded.
-    const int a_row = tid & 127, a_ab = a_row >> 5, w_base = tid >> 7;
-    const int a_j = min(j0 + (a_row & 31), (int)m_pad - 1);
+    constexpr int kAb = kW / 4;
+    const int wA = warp % kW, ab0 = (warp / kW) * kAb, w_base = tid >> 7;
+    const int a_j = min(j0 + lane, (int)m_pad - 1);
     const int b_kl = tid & 127;
     const bool b_on = b_kl < kK;
     const int b_k = k0 + b_kl;
-    const uint32_t offa0 = (a_row >> 3) * kSbo + (a_row & 7) * 16;
     const uint32_t offb0 = (b_kl >> 3) * kSbo + (b_kl & 7) * 16;  // + (kK/8)*kSbo for c = 1
-    auto load_words = [&](int cc, uint2 (&gi)[kU], uint2 (&gj)[kU], uint2 (&gk)[kU]) {
+    auto load_words = [&](int cc, uint2& gi, uint2& gj, uint2 (&gk)[kU]) {
       const bool c1 = cc >= nc0;
       const int c_in = c1 ? cc - nc0 : cc;
       const int wcls = c1 ? jv.w1 : jv.w0;
       const int64_t wb = (c1 ? (int64_t)jv.w0 : 0) + (int64_t)kW * c_in;
+      gi = make_uint2(0, 0);
+      gj = gi;
+      if (kW * c_in + wA < wcls) {
+        const uint2* row = jv.planes + (wb + wA) * m_pad;
+        gi = __ldg(row + i);
+        gj = __ldg(row + a_j);
+      }
 #pragma unroll
       for (int r = 0; r < kU; r++) {
         const int w = w_base + 4 * r;
-        gi[r] = make_uint2(0, 0);
-        gj[r] = gi[r];
-        gk[r] = gi[r];
-        if (kW * c_in + w < wcls) {
-          const uint2* row = jv.planes + (wb + w) * m_pad;
-          gi[r] = __ldg(row + i);
-          gj[r] = __ldg(row + a_j);
-          if (b_on && b_k < m_pad) gk[r] = __ldg(row + b_k);
-        }
+        gk[r] = make_uint2(0, 0);
+        if (kW * c_in + w < wcls && b_on && b_k < m_pad) gk[r] = __ldg(jv.planes + (wb + w) * m_pad + b_k);
       }
     };
     if (worker) {
-      uint2 ci[kU], cj[kU], ck[kU];
+      uint2 ci, cj, ck[kU];
       if (nct > 0) load_words(0, ci, cj, ck);
       for (int cc = 0; cc < nct; ++cc) {
         const uint32_t g = g_chunk + (uint32_t)cc;
-        uint2 ni[kU], nj[kU], nk[kU];
+        uint2 ni = make_uint2(0, 0), nj = ni, nk[kU];
 #pragma unroll
-        for (int r = 0; r < kU; r++) ni[r] = nj[r] = nk[r] = make_uint2(0, 0);
+        for (int r = 0; r < kU; r++) nk[r] = make_uint2(0, 0);
         if (cc + 1 < nct) load_words(cc + 1, ni, nj, nk);
         const int s = (int)(g % kStages);
         const uint32_t use = g / kStages;
@@ -368,20 +370,27 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         if (__shfl_sync(kFull, *abort_flag, 0)) break;  // warp-uniform
         const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
 #pragma unroll
+        for (int t = 0; t < kAb; t++) {
+          const int ab = ab0 + t, row = 32 * ab + lane;
+          const uint32_t wa = ((ab >> 1) ? ci.y : ci.x) & ((ab & 1) ? cj.y : cj.x);
+          const uint32_t offa = sA + (row >> 3) * kSbo + (row & 7) * 16;
+          if (kFp4) {
+            sts128(offa + wA * 128, expand32_fp4(wa));
+          } else {
+            sts128(offa + (2 * wA) * 128, expand16(wa));
+            sts128(offa + (2 * wA) * 128 + 128, expand16(wa >> 16));
+          }
+        }
+#pragma unroll
         for (int r = 0; r < kU; r++) {
           const int w = w_base + 4 * r;
-          const uint32_t wa = ((a_ab >> 1) ? ci[r].y : ci[r].x) & ((a_ab & 1) ? cj[r].y : cj[r].x);
-          if (kFp4) {  // word w = K group w (16 bytes)
-            sts128(sA + offa0 + w * 128, expand32_fp4(wa));
+          if (kFp4) {
             if (b_on) {
               const uint32_t offb = sB + offb0 + w * 128;
               sts128(offb, expand32_fp4(ck[r].x));
               sts128(offb + (kK / 8) * kSbo, expand32_fp4(ck[r].y));
             }
-          } else {  // word w = K groups 2w, 2w+1
-            const uint32_t offa = sA + offa0 + (2 * w) * 128;
-            sts128(offa, expand16(wa));
-            sts128(offa + 128, expand16(wa >> 16));
+          } else {
             const uint32_t offb = sB + offb0 + (2 * w) * 128;
             sts128(offb, expand16(ck[r].x));
             sts128(offb + 128, expand16(ck[r].x >> 16));
@@ -389,12 +398,10 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
             sts128(offb + (kK / 8) * kSbo + 128, expand16(ck[r].y >> 16));
           }
         }
+        ci = ni;
+        cj = nj;
 #pragma unroll
-        for (int r = 0; r < kU; r++) {
-          ci[r] = ni[r];
-          cj[r] = nj[r];
-          ck[r] = nk[r];
-        }
+        for (int r = 0; r < kU; r++) ck[r] = nk[r];
         fence_proxy_async();
         __syncwarp();
         if (lane == 0) bar_arrive(bar_full0 + 8 * s);
