@@ -27,6 +27,7 @@ struct epik2_ctx {
   int32_t next_id = 1;
   // search scratch
   int engine = 0;               // default engine: 0 = auto, 1 = integer, 2 = tensor cores int8, 3 = tensor cores FP4
+  int stage_words = 0;          // default tensor-core stage depth: 0 = autotuned
   int scan_blocks = 0;          // integer engine grid
   int tc_blocks = 0;            // tensor-core engine grid (one CTA per SM)
   int n_slots = 0;              // per-warp slots, enough for either grid
@@ -248,7 +249,7 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   if (ie < ib) ie = ib;
   int engine = ctx->engine;
   if (opts && opts->engine != 0) engine = opts->engine;
-  int kw = (opts && opts->stage_words) ? opts->stage_words : 0;
+  int kw = (opts && opts->stage_words) ? opts->stage_words : ctx->stage_words;
   if (engine == EPIK2_ENGINE_TC_FP4 && !fp4_exact(d))
     return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
   if (engine == 0 || ((engine == 2 || engine == 3) && kw == 0)) {
@@ -384,10 +385,13 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   const int64_t m = d.n_snps;
   const int64_t kk = tc_k_per_tile(fp4);
   const int64_t n_kb = (m + kk - 1) / kk;
+  const bool pair = tc_pair(fp4, kw);
+  const int64_t jstep = pair ? 64 : 32;  // SNPs j per tile (a CTA pair takes 64)
+  const int grid = pair ? tc_pair_blocks(ctx->tc_blocks) : ctx->tc_blocks;
   std::vector<uint32_t> ij;
   std::vector<int64_t> off(1, 0);
   for (int64_t i = ib; i < ie; i++)
-    for (int64_t j0 = i + 1; j0 <= m - 2; j0 += 32) {
+    for (int64_t j0 = i + 1; j0 <= m - 2; j0 += jstep) {
       ij.push_back((uint32_t)i);
       ij.push_back((uint32_t)j0);
       off.push_back(off.back() + (n_kb - (j0 + 1) / kk));
@@ -431,9 +435,9 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   p.dump_scores = dump_scores;
   p.err = ctx->d_err;
   CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
-  CK(ctx, launch_scan_tc(p, ctx->tc_blocks, kw, fp4, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
+  CK(ctx, launch_scan_tc(p, grid, kw, fp4, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
   CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
-  const int n_warps = ctx->tc_blocks * tc_warps_per_block();
+  const int n_warps = grid * tc_warps_per_block();
   CK(ctx, launch_reduce_best(ctx->d_slots, n_warps, ctx->d_best, ctx->stream), "reduce kernel");
   ctx->stats.kernel_launches += 2;
   CK(ctx, cudaMemcpyAsync(ctx->h_best, ctx->d_best, sizeof(BestSlot), cudaMemcpyDeviceToHost, ctx->stream),
@@ -581,19 +585,20 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     for (int32_t b = 0; b < n; b++) {
       const bool fp4 = codes[b] & 1;
       const int64_t m = ds[b]->n_snps, kk = tc_k_per_tile(fp4), n_kb = (m + kk - 1) / kk;
-      auto li = lists.find({m, kk});
+      const int64_t jstep = tc_pair(fp4, codes[b] >> 1) ? 64 : 32;
+      auto li = lists.find({m, kk * 2 + (jstep == 64 ? 1 : 0)});
       if (li == lists.end()) {
         ListInfo L{(int64_t)pb_off_all.size(), (int64_t)pb_ij_all.size(), 0, 0};
         pb_off_all.push_back(0);
         for (int64_t i = 0; i < m; i++)
-          for (int64_t j0 = i + 1; j0 <= m - 2; j0 += 32) {
+          for (int64_t j0 = i + 1; j0 <= m - 2; j0 += jstep) {
             pb_ij_all.push_back((uint32_t)i);
             pb_ij_all.push_back((uint32_t)j0);
             L.tiles += n_kb - (j0 + 1) / kk;
             pb_off_all.push_back(L.tiles);
             L.n_pb++;
           }
-        li = lists.emplace(std::make_pair(m, kk), L).first;
+        li = lists.emplace(std::make_pair(m, kk * 2 + (jstep == 64 ? 1 : 0)), L).first;
       }
       job_pb_base[b] = li->second.off_base;
       job_ij_base[b] = li->second.ij_base;
@@ -664,7 +669,9 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
       p.n_jobs = n;
       p.job_slots = pl->d_job_slots;
       p.n_tiles = nt;
-      e = launch_scan_tc(p, grid, group_code[g] >> 1, group_code[g] & 1, false, ctx->stream);
+      const bool gp = tc_pair(group_code[g] & 1, group_code[g] >> 1);
+      e = launch_scan_tc(p, gp ? tc_pair_blocks(grid) : grid, group_code[g] >> 1, group_code[g] & 1, false,
+                         ctx->stream);
     }
     if (e == cudaSuccess) e = launch_reduce_jobs(pl->d_job_slots, n, grid, pl->d_results, ctx->stream);
     if (e == cudaSuccess && rescore) e = launch_rescore_jobs(pl->d_jobs, pl->d_results, n, pl->d_resc, ctx->stream);
@@ -826,6 +833,14 @@ int epik2_set_engine(epik2_ctx* ctx, int engine) {
   if (!ctx) return EPIK2_E_INVALID;
   if (engine < EPIK2_ENGINE_AUTO || engine > EPIK2_ENGINE_TC_FP4) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
   ctx->engine = engine;
+  return EPIK2_OK;
+}
+
+int epik2_set_stage_words(epik2_ctx* ctx, int stage_words) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (stage_words != 0 && stage_words != 4 && stage_words != 8 && stage_words != 16)
+    return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4, 8 or 16");
+  ctx->stage_words = stage_words;
   return EPIK2_OK;
 }
 

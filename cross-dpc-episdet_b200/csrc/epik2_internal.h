@@ -135,6 +135,9 @@ int scan_blocks_per_sm();
 cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool dump,
                            cudaStream_t stream);
 int tc_k_per_tile(bool fp4);  // SNPs k per tensor-core tile: 128 (int8) or 112 (FP4)
+// FP4 at 16 words per stage runs as CTA pairs (clusters of two, tiles of 64 pairs j).
+bool tc_pair(bool fp4, int words_per_stage);
+int tc_pair_blocks(int sms);  // resident CTAs of the CTA-pair kernel (even)
 // Tile descriptors of one pair-block list (prefix sums pb_off[0..n_pb], (i, j0) pairs) into
 // out[pb_off[b] ...], tagged with `job`.
 cudaError_t launch_expand_tiles(const int64_t* pb_off, const uint32_t* pb_ij, int64_t n_pb, bool fp4, int job,

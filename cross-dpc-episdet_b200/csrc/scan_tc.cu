@@ -28,6 +28,7 @@
 //
 // Every wait on an mbarrier is bounded (about 2 s of SM clock); on expiry the kernel sets
 // an error word, stops taking tiles, frees its tensor memory and returns.
+#include <algorithm>
 #include <cfloat>
 
 #include "epik2_internal.h"
@@ -47,6 +48,8 @@ constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) 
 // block-scaled instruction descriptor (kind::mxf4): A/B E2M1, scale factors UE8M0, both
 // K-major, N = 224, M = 128, K = 64, scale-factor byte selectors 0.  D is FP32.
 constexpr uint32_t kIdescFp4 = (1u << 7) | (1u << 10) | ((224u >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
+// the same for a CTA pair (cta_group::2): M = 256, each CTA holding 128 rows of A, 112 of B
+constexpr uint32_t kIdescFp4Pair = (1u << 7) | (1u << 10) | ((224u >> 3) << 17) | (1u << 23) | ((256u >> 4) << 24);
 // FP4 format: TMEM columns [224, 256) hold the scale factors (all 2^1), A's from 224 (4
 // columns), B's from 240 (8 columns); class 0 accumulates into [0, 224), class 1 into
 // [256, 480).
@@ -92,6 +95,46 @@ __device__ __forceinline__ void tmem_st16_fill(uint32_t addr, uint32_t v) {
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
+// CTA-pair forms.  The MMA is issued by the even CTA of a cluster of two; each CTA's shared
+// memory holds its half of A and of B at the same offsets, and each CTA's tensor memory
+// receives its 128 rows of D.
+__device__ __forceinline__ void mma_fp4_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate,
+                                             uint32_t sfa_tmem, uint32_t sfb_tmem) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::mxf4.block_scale.scale_vec::2X [%0], %1, %2, %3, [%5], [%6], p;\n\t}\n" ::"r"(
+          d_tmem),
+      "l"(a), "l"(b), "r"(kIdescFp4Pair), "r"(accumulate), "r"(sfa_tmem), "r"(sfb_tmem));
+}
+// arrive on the mbarrier at this offset in both CTAs of the pair once the MMAs complete
+__device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(bar),
+      "h"((uint16_t)3)
+      : "memory");
+}
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// address of the same shared-memory offset in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t map_cta(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void bar_arrive_cluster(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ void st_cluster_s64(uint32_t cluster_addr, long long v) {
+  asm volatile("st.shared::cluster.b64 [%0], %1;" ::"r"(cluster_addr), "l"(v) : "memory");
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
@@ -114,6 +157,23 @@ __device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity) {
       : "r"(bar), "r"(parity)
       : "memory");
   return ok != 0;
+}
+
+// Bounded wait with cluster-scope acquire (arrivals come from the other CTA of a pair).
+__device__ __forceinline__ bool bar_wait_cluster(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > kWaitLimit) return false;
+  }
 }
 
 // Bounded wait for the completion of the mbarrier phase with the given parity.
@@ -189,14 +249,19 @@ struct JobView {
 // per stage: 4 stages of 48 KiB or 2 of 96 KiB) or E2M1 (kind::mxf4, 112 SNPs k per tile so
 // that the scale factors fit in tensor memory beside the two accumulators, kW = 8 or 16:
 // 4 stages of 44 KiB or 2 of 88 KiB).  kW = class words (32 samples each) per stage.
+// kPair (FP4 only): a cluster of two CTAs computes one tile of 64 pairs (M = 256,
+// cta_group::2): CTA r holds the A rows of pairs j0+32r.. and the B rows of g_k = r, so each
+// CTA expands 128 + 112 operand rows per stage instead of 128 + 224; the even CTA issues.
 // kBatched: tiles of many datasets on one queue, per-dataset results.
-template <int kW, bool kFp4, bool kBatched, bool kDump, bool kTopK>
+template <int kW, bool kFp4, bool kPair, bool kBatched, bool kDump, bool kTopK>
 __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) {
+  static_assert(!kPair || kFp4, "CTA pairs use the FP4 format");
   constexpr int kK = kFp4 ? 112 : 128;                // SNPs k per tile -> 2*kK rows of B
   constexpr int kRowBytes = (kFp4 ? 16 : 32) * kW;    // operand bytes per row per stage
+  constexpr int kBRows = kPair ? kK : 2 * kK;         // B rows held by this CTA
   constexpr int kStageA = 128 * kRowBytes;
-  constexpr int kStageBytes = (128 + 2 * kK) * kRowBytes;
-  constexpr int kStages = kRingBytes / kStageBytes;
+  constexpr int kStageBytes = (128 + kBRows) * kRowBytes;
+  constexpr int kStages = (kRingBytes / kStageBytes) < 4 ? (kRingBytes / kStageBytes) : 4;
   constexpr uint32_t kSbo = 8 * kRowBytes;            // bytes between 8-row groups
   constexpr int kMmas = kFp4 ? kW / 2 : kW;           // MMAs per stage (K = 64 E2M1 or 32 int8)
   constexpr int kU = kW / 4;                          // units of each kind per thread per stage
@@ -212,22 +277,35 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   const uint32_t stage0 = smem_u32(smem);
   const uint32_t bar0 = smem_u32(bars);
   const uint32_t bar_acc = bar0 + 8 * kStages;
-  const uint32_t bar_full0 = bar_acc + 8;  // [stages]: one arrival per producing warp
+  const uint32_t bar_full0 = bar_acc + 8;  // [stages]: one arrival per producing warp (+1 forwarded)
+  const uint32_t bar_tile = bar_full0 + 8 * kStages;  // CTA pairs: the odd CTA's "next tile is set"
   volatile int* abort_flag = &s_abort;
   const bool worker = warp < kTcWarps;
+  const uint32_t crank = kPair ? cluster_rank() : 0u;  // rank in the CTA pair
+  const bool issuer_cta = crank == 0;
 
   if (tid == 0) {
     for (int s = 0; s < kStages; s++) bar_init(bar0 + 8 * s, 1);
     bar_init(bar_acc, 1);
-    for (int s = 0; s < kStages; s++) bar_init(bar_full0 + 8 * s, kTcWarps);
+    // full: the CTA's producing warps, and in a pair's issuing CTA one forwarded arrival
+    for (int s = 0; s < kStages; s++) bar_init(bar_full0 + 8 * s, kTcWarps + ((kPair && crank == 0) ? 1 : 0));
+    bar_init(bar_tile, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
   }
+  if (kPair) cluster_sync_all();  // the pair's barriers are initialised before any remote arrival
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                 "r"(512u)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    if (kPair) {
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                   "r"(512u)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                   "r"(512u)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -242,6 +320,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     }
     tc_fence_before();
     __syncthreads();
+    if (kPair) cluster_sync_all();  // both CTAs' scale factors are in place before the first MMA
     tc_fence_after();
   }
 
@@ -249,7 +328,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   unsigned long long best_k = ~0ull;
   float list_s = FLT_MAX;
   unsigned long long list_k = ~0ull;
-  uint32_t g_chunk = 0, n_tile = 0;
+  uint32_t g_chunk = 0, n_tile = 0, n_fetch = 0;
   const uint32_t* E = reinterpret_cast<const uint32_t*>(smem);  // epilogue staging, reuses the stages
 
   // Batched form: fold the CTA's candidates for dataset jb into its slot of that dataset.
@@ -294,9 +373,20 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     // next tile from the shared queue; its descriptor (one 8-byte load) gives the dataset,
     // the first index, the pair block and the k block
     if (tid == 0) {
-      const unsigned long long t = atomicAdd(p.counter, 1ull);
-      s_tile = (t < (unsigned long long)p.n_tiles && !s_abort) ? (long long)__ldg(p.tiles + t) : -1ll;
+      if (issuer_cta) {
+        const unsigned long long t = atomicAdd(p.counter, 1ull);
+        const long long d = (t < (unsigned long long)p.n_tiles && !s_abort) ? (long long)__ldg(p.tiles + t) : -1ll;
+        s_tile = d;
+        if (kPair) {  // hand the tile to the odd CTA: store, then release-arrive on its barrier
+          st_cluster_s64(map_cta(smem_u32(&s_tile), 1), d);
+          bar_arrive_cluster(map_cta(bar_tile, 1));
+        }
+      } else if (!bar_wait_cluster(bar_tile, n_fetch & 1u)) {
+        s_abort = 1;
+        s_tile = -1;
+      }
     }
+    ++n_fetch;
     __syncthreads();
     const long long desc = s_tile;
     if (kBatched) {  // desc is the same for every thread: the flush is uniform
@@ -307,7 +397,8 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       }
     }
     if (desc < 0) break;
-    const int i = tile_i(desc), j0 = tile_j0(desc), k0 = kK * tile_kb(desc);
+    // this CTA's pairs: j0 .. j0+31 (pairs of a CTA pair: 32*rank further)
+    const int i = tile_i(desc), j0 = tile_j0(desc) + 32 * (int)crank, k0 = kK * tile_kb(desc);
     const int job = kBatched ? tile_job(desc) : 0;
     JobView jv;
     if (kBatched) {
@@ -351,7 +442,12 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       for (int r = 0; r < kU; r++) {
         const int w = w_base + 4 * r;
         gk[r] = make_uint2(0, 0);
-        if (kW * c_in + w < wcls && b_on && b_k < m_pad) gk[r] = __ldg(jv.planes + (wb + w) * m_pad + b_k);
+        if (kW * c_in + w < wcls && b_on && b_k < m_pad) {
+          if (kPair)  // this CTA's B rows: g_k = rank only
+            gk[r].x = __ldg(reinterpret_cast<const uint32_t*>(jv.planes + (wb + w) * m_pad + b_k) + crank);
+          else
+            gk[r] = __ldg(jv.planes + (wb + w) * m_pad + b_k);
+        }
       }
     };
     if (worker) {
@@ -365,7 +461,8 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         if (cc + 1 < nct) load_words(cc + 1, ni, nj, nk);
         const int s = (int)(g % kStages);
         const uint32_t use = g / kStages;
-        const bool late = use > 0 && !bar_wait(bar0 + 8 * s, (use & 1u) ^ 1u);
+        const bool late =
+            use > 0 && !(kPair ? bar_wait_cluster(bar0 + 8 * s, (use & 1u) ^ 1u) : bar_wait(bar0 + 8 * s, (use & 1u) ^ 1u));
         if (__any_sync(kFull, late)) *abort_flag = 1;
         if (__shfl_sync(kFull, *abort_flag, 0)) break;  // warp-uniform
         const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
@@ -384,7 +481,9 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
 #pragma unroll
         for (int r = 0; r < kU; r++) {
           const int w = w_base + 4 * r;
-          if (kFp4) {
+          if (kPair) {
+            if (b_on) sts128(sB + offb0 + w * 128, expand32_fp4(ck[r].x));
+          } else if (kFp4) {
             if (b_on) {
               const uint32_t offb = sB + offb0 + w * 128;
               sts128(offb, expand32_fp4(ck[r].x));
@@ -406,13 +505,25 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         __syncwarp();
         if (lane == 0) bar_arrive(bar_full0 + 8 * s);
       }
-    } else if (lane == 0) {
+    } else if (kPair && lane == 0 && !issuer_cta) {
+      // the odd CTA of a pair forwards "stage stored" to the issuing CTA: one cluster-scope
+      // arrival per stage once all its producing warps have arrived locally
+      for (int cc = 0; cc < nct; ++cc) {
+        const uint32_t g = g_chunk + (uint32_t)cc;
+        const int s = (int)(g % kStages);
+        if (!bar_wait(bar_full0 + 8 * s, (g / kStages) & 1u)) {
+          *abort_flag = 1;
+          break;
+        }
+        bar_arrive_cluster(map_cta(bar_full0 + 8 * s, 0));
+      }
+    } else if (lane == 0 && issuer_cta) {
       // the issuing warp: wait for each stage's operands, issue its MMAs, release it
       for (int cc = 0; cc < nct; ++cc) {
         const uint32_t g = g_chunk + (uint32_t)cc;
         const int s = (int)(g % kStages);
         const uint32_t use = g / kStages;
-        if (!bar_wait(bar_full0 + 8 * s, use & 1u)) {
+        if (!(kPair ? bar_wait_cluster(bar_full0 + 8 * s, use & 1u) : bar_wait(bar_full0 + 8 * s, use & 1u))) {
           *abort_flag = 1;
           break;
         }
@@ -425,13 +536,20 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
 #pragma unroll
         for (int kk = 0; kk < kMmas; kk++) {  // each MMA reads 32 bytes of every row: 256 B on
           const uint32_t acc = (c_in > 0 || kk > 0) ? 1u : 0u;
-          if (kFp4)
+          if (kPair)
+            mma_fp4_pair(d, da + (uint64_t)(16 * kk), db + (uint64_t)(16 * kk), acc, tmem + kSfaCol, tmem + kSfbCol);
+          else if (kFp4)
             mma_fp4(d, da + (uint64_t)(16 * kk), db + (uint64_t)(16 * kk), acc, tmem + kSfaCol, tmem + kSfbCol);
           else
             mma_i8(d, da + (uint64_t)(16 * kk), db + (uint64_t)(16 * kk), acc);
         }
-        mma_commit(bar0 + 8 * s);
-        if (cc == nct - 1) mma_commit(bar_acc);
+        if (kPair) {
+          mma_commit_pair(bar0 + 8 * s);
+          if (cc == nct - 1) mma_commit_pair(bar_acc);
+        } else {
+          mma_commit(bar0 + 8 * s);
+          if (cc == nct - 1) mma_commit(bar_acc);
+        }
       }
     }
     g_chunk += (uint32_t)nct;
@@ -441,7 +559,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
 
     // ---- epilogue: TMEM -> shared -> complete tables, score, select ----
     {
-      const bool ok = bar_wait(bar_acc, n_tile & 1u);
+      const bool ok = kPair ? bar_wait_cluster(bar_acc, n_tile & 1u) : bar_wait(bar_acc, n_tile & 1u);
       if (!ok) *abort_flag = 1;
       __syncthreads();
       if (*abort_flag) break;
@@ -558,9 +676,13 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   tc_fence_before();
   __syncthreads();
   if (s_abort && tid == 0) atomicExch(p.err, 1);
+  if (kPair) cluster_sync_all();  // the pair's MMAs and remote arrivals are over
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+    if (kPair)
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+    else
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
   }
   if (!kBatched && worker) {
 #pragma unroll
@@ -662,28 +784,28 @@ __global__ void k_fill_slots(BestSlot* __restrict__ slots, int64_t n) {
 
 int tc_warps_per_block() { return kTcWarps; }
 
-template <int kW, bool kF, bool kB, bool kD, bool kT>
+template <int kW, bool kF, bool kP, bool kB, bool kD, bool kT>
 static cudaError_t set_smem() {
-  return cudaFuncSetAttribute(k_scan_tc<kW, kF, kB, kD, kT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_scan_tc<kW, kF, kP, kB, kD, kT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kTcSmemBytes);
 }
 
-template <int kW, bool kF>
+template <int kW, bool kF, bool kP>
 static cudaError_t set_smem_all() {
-  cudaError_t e = set_smem<kW, kF, false, false, false>();
-  if (e == cudaSuccess) e = set_smem<kW, kF, false, true, false>();
-  if (e == cudaSuccess) e = set_smem<kW, kF, false, false, true>();
-  if (e == cudaSuccess) e = set_smem<kW, kF, true, false, false>();
+  cudaError_t e = set_smem<kW, kF, kP, false, false, false>();
+  if (e == cudaSuccess) e = set_smem<kW, kF, kP, false, true, false>();
+  if (e == cudaSuccess) e = set_smem<kW, kF, kP, false, false, true>();
+  if (e == cudaSuccess) e = set_smem<kW, kF, kP, true, false, false>();
   return e;
 }
 
 cudaError_t tc_configure() {
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = set_smem_all<4, false>();
-    if (e == cudaSuccess) e = set_smem_all<8, false>();
-    if (e == cudaSuccess) e = set_smem_all<8, true>();
-    if (e == cudaSuccess) e = set_smem_all<16, true>();
+    cudaError_t e = set_smem_all<4, false, false>();
+    if (e == cudaSuccess) e = set_smem_all<8, false, false>();
+    if (e == cudaSuccess) e = set_smem_all<8, true, false>();
+    if (e == cudaSuccess) e = set_smem_all<16, true, true>();
     if (e != cudaSuccess) return e;
     configured = true;
   }
@@ -692,13 +814,61 @@ cudaError_t tc_configure() {
 
 template <int kW, bool kF>
 static void launch_variant(const TcParams& p, int blocks, bool batched, bool dump, bool topk, cudaStream_t stream) {
-  if (batched) k_scan_tc<kW, kF, true, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
-  else if (dump) k_scan_tc<kW, kF, false, true, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
-  else if (topk) k_scan_tc<kW, kF, false, false, true><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
-  else k_scan_tc<kW, kF, false, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+  if (batched) k_scan_tc<kW, kF, false, true, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+  else if (dump) k_scan_tc<kW, kF, false, false, true, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+  else if (topk) k_scan_tc<kW, kF, false, false, false, true><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+  else k_scan_tc<kW, kF, false, false, false, false><<<blocks, kTcThreadsAll, kTcSmemBytes, stream>>>(p);
+}
+
+// CTA-pair kernels: clusters of two CTAs
+template <bool kB, bool kD, bool kT>
+static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t stream) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)blocks);
+  cfg.blockDim = dim3(kTcThreadsAll);
+  cfg.dynamicSmemBytes = kTcSmemBytes;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_scan_tc<16, true, true, kB, kD, kT>, p);
 }
 
 int tc_k_per_tile(bool fp4) { return fp4 ? 112 : 128; }
+
+bool tc_pair(bool fp4, int words_per_stage) { return fp4 && words_per_stage == 16; }
+
+// CTAs of the CTA-pair kernel that can be resident at once (even; at most one per SM).
+int tc_pair_blocks(int sms) {
+  static int blocks = -1;
+  if (blocks < 0) {
+    blocks = sms & ~1;
+    if (tc_configure() == cudaSuccess) {
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3((unsigned)(sms & ~1));
+      cfg.blockDim = dim3(kTcThreadsAll);
+      cfg.dynamicSmemBytes = kTcSmemBytes;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = 2;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, k_scan_tc<16, true, true, false, false, false>, &cfg) ==
+              cudaSuccess &&
+          clusters > 0)
+        blocks = std::min(blocks, 2 * clusters);
+    }
+    cudaGetLastError();
+  }
+  return blocks;
+}
 
 cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool dump,
                            cudaStream_t stream) {
@@ -706,9 +876,15 @@ cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, b
   if (ce != cudaSuccess) return ce;
   const bool topk = p.top_k > 1;
   const bool batched = p.jobs != nullptr;
-  if (fp4) {
-    if (words_per_stage == 16) launch_variant<16, true>(p, blocks, batched, dump, topk, stream);
-    else launch_variant<8, true>(p, blocks, batched, dump, topk, stream);
+  if (tc_pair(fp4, words_per_stage)) {
+    cudaError_t e;
+    if (batched) e = launch_pair<true, false, false>(p, blocks & ~1, stream);
+    else if (dump) e = launch_pair<false, true, false>(p, blocks & ~1, stream);
+    else if (topk) e = launch_pair<false, false, true>(p, blocks & ~1, stream);
+    else e = launch_pair<false, false, false>(p, blocks & ~1, stream);
+    if (e != cudaSuccess) return e;
+  } else if (fp4) {
+    launch_variant<8, true>(p, blocks, batched, dump, topk, stream);
   } else {
     if (words_per_stage == 8) launch_variant<8, false>(p, blocks, batched, dump, topk, stream);
     else launch_variant<4, false>(p, blocks, batched, dump, topk, stream);

@@ -144,6 +144,7 @@ def library():
         "epik2_reset_stats": ([p], ctypes.c_int),
         "epik2_scan_u8_noalloc": ([p, p, i64, i64, p, ctypes.POINTER(Best)], ctypes.c_int),
         "epik2_set_engine": ([p, ctypes.c_int], ctypes.c_int),
+        "epik2_set_stage_words": ([p, ctypes.c_int], ctypes.c_int),
         "epik2_scan_batch": ([p, p, i32, ctypes.POINTER(Opts), ctypes.POINTER(Best)], ctypes.c_int),
         "epik2_autotune": ([p, i32, ctypes.POINTER(Tune)], ctypes.c_int),
         "epik2_load_replicate": ([p, i32, p, ctypes.POINTER(i32)], ctypes.c_int),
@@ -236,7 +237,7 @@ def n_triplets(m):
 class Context:
     """One device context: owns a CUDA stream and the resident datasets."""
 
-    def __init__(self, device=0, engine=ENGINE_AUTO):
+    def __init__(self, device=0, engine=ENGINE_AUTO, stage_words=0):
         self._lib = library()
         h = ctypes.c_void_p()
         r = self._lib.epik2_create(ctypes.byref(h), device)
@@ -245,6 +246,8 @@ class Context:
         self._h = h
         if engine:
             self.set_engine(engine)
+        if stage_words:
+            self._check(self._lib.epik2_set_stage_words(self._h, stage_words))
 
     def close(self):
         if getattr(self, "_h", None):

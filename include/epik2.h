@@ -102,6 +102,10 @@ int epik2_mem_info(const epik2_ctx *ctx, size_t *free_bytes, size_t *total_bytes
                                  accumulators: exact while every class has < 2^24 samples,
                                  else EPIK2_E_TOO_LARGE */
 int epik2_set_engine(epik2_ctx *ctx, int engine);
+/* Default tensor-core stage depth of the context (used when epik2_opts.stage_words is 0):
+ * 0 = autotuned, else 4 or 8 (int8) / 8 or 16 (FP4; 16 runs as clusters of two CTAs that
+ * share one 64-pair tile). */
+int epik2_set_stage_words(epik2_ctx *ctx, int stage_words);
 
 /* Run the context's work on a caller-owned stream (e.g. a PyTorch stream); NULL restores
  * the context's own stream.  The library still synchronises that stream before it

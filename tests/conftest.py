@@ -59,12 +59,12 @@ def pytest_collection_modifyitems(config, items):
 ENGINES = {1: "int", 2: "tc", 3: "fp4"}
 
 
-@pytest.fixture(scope="session", params=[1, 2, 3], ids=["int", "tc", "fp4"])
+@pytest.fixture(scope="session", params=[(1, 0), (2, 0), (3, 8), (3, 16)], ids=["int", "tc", "fp4", "fp4pair"])
 def ctx(request):
     """A device context per search engine (integer pipe, int8 tensor cores, FP4 tensor
-    cores): every test that takes `ctx` runs on all three."""
+    cores, FP4 tensor cores on CTA pairs): every test that takes `ctx` runs on all four."""
     import epik2
-    c = epik2.Context(0, engine=request.param)
+    c = epik2.Context(0, engine=request.param[0], stage_words=request.param[1])
     yield c
     c.close()
 
