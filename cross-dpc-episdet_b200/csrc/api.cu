@@ -397,6 +397,20 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
       off.push_back(off.back() + (n_kb - (j0 + 1) / kk));
     }
   const int64_t n_pb = (int64_t)off.size() - 1;
+  if (n_pb > ctx->pb_cap || off.back() > ctx->tiles_cap) {
+    // grow once to the whole search of this dataset, so that its shards never reallocate
+    // (a reallocation synchronises the device)
+    int64_t all_pb = 0, all_tiles = 0;
+    for (int64_t i = 0; i < m; i++)
+      for (int64_t j0 = i + 1; j0 <= m - 2; j0 += jstep) {
+        all_pb++;
+        all_tiles += n_kb - (j0 + 1) / kk;
+      }
+    int r0 = ensure_pb(ctx, std::max<int64_t>(all_pb, 1));
+    if (r0) return r0;
+    r0 = ensure_tiles(ctx, std::max<int64_t>(all_tiles, 1));
+    if (r0) return r0;
+  }
   int r = ensure_pb(ctx, std::max<int64_t>(n_pb, 1));
   if (r) return r;
   r = ensure_tiles(ctx, std::max<int64_t>(off.back(), 1));
