@@ -11,8 +11,9 @@ triplet scored over one sample.
 A step scans one shard of the triplet space: the first SNP index i is cut into
 `--shards` contiguous ranges of equal work (C(M-1-i, 2) triplets per i); step t of
 rank r scans shard (t*N + r) mod shards, so K = shards steps on one GPU cover every
-triplet once.  Per-GPU work is fixed as N grows ("weak" scaling; the only exchange
-of a sharded search is the final argmin, which is outside the timed steps).
+triplet once.  Per-GPU work is fixed as N grows ("weak" scaling).  The one exchange of
+a sharded search, the argmin over ranks (two MIN all-reduces of one int64), closes every
+step when N > 1.
 
 Our arm ("value") runs with the dataset resident in HBM; "e2e" repeats the steps
 through the public one-call entry point (epik2_scan_u8) from pinned host buffers, so
@@ -193,6 +194,12 @@ def run_ours(args, rank, world, local_rank):
     shards = SH.shard_bounds(M, parts)
     peaks = epik2.probe_int_peaks(local_rank)
     tune = ctx.autotune(did)  # AUTO-engine scans below use this choice
+    if args.engine != "auto":  # a pinned engine (profiling runs): report it as the choice
+        ctx.set_engine({"int": epik2.ENGINE_INT, "tc": epik2.ENGINE_TC, "fp4": epik2.ENGINE_TC_FP4}[args.engine])
+        tune = dict(tune, engine={"int": epik2.ENGINE_INT, "tc": epik2.ENGINE_TC, "fp4": epik2.ENGINE_TC_FP4}[args.engine])
+    if args.stage_words:
+        ctx.set_stage_words(args.stage_words)
+        tune = dict(tune, stage_words=args.stage_words)
     engine_tc = tune["engine"] in (epik2.ENGINE_TC, epik2.ENGINE_TC_FP4)
     engine_fp4 = tune["engine"] == epik2.ENGINE_TC_FP4
     flush = torch.empty(args.flush_mb << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
@@ -583,6 +590,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "precision", "serving"])
+    ap.add_argument("--engine", default="auto", choices=["auto", "int", "tc", "fp4"],
+                    help="plain form: search engine (default: the autotuner's choice)")
+    ap.add_argument("--stage-words", type=int, default=0, help="plain form: tensor-core stage depth (0 = tuned)")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-drain", type=float, default=30.0)
     args = ap.parse_args()

@@ -247,7 +247,7 @@ class Context:
         if engine:
             self.set_engine(engine)
         if stage_words:
-            self._check(self._lib.epik2_set_stage_words(self._h, stage_words))
+            self.set_stage_words(stage_words)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -276,8 +276,12 @@ class Context:
         return self._h
 
     def set_engine(self, engine):
-        """Default engine of this context: ENGINE_AUTO, ENGINE_INT or ENGINE_TC."""
+        """Default engine of this context: ENGINE_AUTO, ENGINE_INT, ENGINE_TC or ENGINE_TC_FP4."""
         self._check(self._lib.epik2_set_engine(self._h, engine))
+
+    def set_stage_words(self, stage_words):
+        """Default tensor-core stage depth (0 = autotuned; int8 4/8, FP4 8/16)."""
+        self._check(self._lib.epik2_set_stage_words(self._h, stage_words))
 
     def stats(self):
         st = Stats()
