@@ -5,6 +5,10 @@
 //   epik2_v4 --file <geno.bin> <num_samples> <num_snps>   (matrix + phenotype from a file:
 //                                                          n*m genotype bytes, sample-major,
 //                                                          then n phenotype bytes)
+//   epik2_v4 --plink <prefix> [missing_genotype]          (PLINK 1 binary fileset
+//                                                          <prefix>.bed/.bim/.fam; missing
+//                                                          genotypes read as the given value,
+//                                                          default 0)
 //
 // With positional arguments the data is the reference's own synthetic input
 // (srand(100) generator, GPU/v4.cpp:81-110) and the output has the reference's lines
@@ -28,8 +32,9 @@
 static int usage(const char* argv0) {
   std::fprintf(stderr,
                "usage: %s <num_samples> <num_snps> [block_size]\n"
-               "       %s --file <geno.bin> <num_samples> <num_snps>\n",
-               argv0, argv0);
+               "       %s --file <geno.bin> <num_samples> <num_snps>\n"
+               "       %s --plink <prefix> [missing_genotype]\n",
+               argv0, argv0, argv0);
   return 2;
 }
 
@@ -37,7 +42,24 @@ int main(int argc, char** argv) {
   if (argc < 3) return usage(argv[0]);
   long long n = 0, m = 0;
   std::vector<uint8_t> geno, pheno;
-  if (std::strcmp(argv[1], "--file") == 0) {
+  if (std::strcmp(argv[1], "--plink") == 0) {
+    int64_t ns = 0, ms = 0;
+    int r = epik2_plink_dims(argv[2], &ns, &ms);
+    if (r != EPIK2_OK || ns < 1 || ms < 3) {
+      std::fprintf(stderr, "cannot read PLINK fileset %s: %s\n", argv[2], epik2_strerror(r ? r : EPIK2_E_INVALID));
+      return 1;
+    }
+    n = ns;
+    m = ms;
+    geno.resize((size_t)(n * m));
+    pheno.resize((size_t)n);
+    const int missing = argc > 3 ? std::atoi(argv[3]) : 0;
+    r = epik2_read_plink(argv[2], (uint8_t)missing, geno.data(), pheno.data());
+    if (r != EPIK2_OK) {
+      std::fprintf(stderr, "cannot read PLINK fileset %s: %s\n", argv[2], epik2_strerror(r));
+      return 1;
+    }
+  } else if (std::strcmp(argv[1], "--file") == 0) {
     if (argc < 5) return usage(argv[0]);
     n = std::atoll(argv[3]);
     m = std::atoll(argv[4]);

@@ -145,6 +145,10 @@ def library():
         "epik2_scan_u8_noalloc": ([p, p, i64, i64, p, ctypes.POINTER(Best)], ctypes.c_int),
         "epik2_set_engine": ([p, ctypes.c_int], ctypes.c_int),
         "epik2_set_stage_words": ([p, ctypes.c_int], ctypes.c_int),
+        "epik2_plink_dims": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
+                             ctypes.c_int),
+        "epik2_read_plink": ([ctypes.c_char_p, ctypes.c_uint8, p, p], ctypes.c_int),
+        "epik2_perm_pvalue": ([ctypes.c_float, p, ctypes.c_int64], ctypes.c_double),
         "epik2_scan_batch": ([p, p, i32, ctypes.POINTER(Opts), ctypes.POINTER(Best)], ctypes.c_int),
         "epik2_autotune": ([p, i32, ctypes.POINTER(Tune)], ctypes.c_int),
         "epik2_load_replicate": ([p, i32, p, ctypes.POINTER(i32)], ctypes.c_int),
@@ -228,6 +232,27 @@ def k2_lut(n_max):
 
 def dataset_bytes(n_samples, n_snps):
     return int(library().epik2_dataset_bytes(n_samples, n_snps))
+
+
+def read_plink(prefix, missing_genotype=0):
+    """PLINK 1 binary fileset -> (geno uint8 [samples, SNPs], pheno uint8 [samples])."""
+    L = library()
+    n, m = ctypes.c_int64(), ctypes.c_int64()
+    r = L.epik2_plink_dims(prefix.encode(), ctypes.byref(n), ctypes.byref(m))
+    if r:
+        raise Epik2Error(r, f"{strerror(r)}: {prefix}")
+    geno = np.zeros((n.value, m.value), dtype=np.uint8)
+    pheno = np.zeros(n.value, dtype=np.uint8)
+    r = L.epik2_read_plink(prefix.encode(), missing_genotype, _ptr(geno), _ptr(pheno))
+    if r:
+        raise Epik2Error(r, f"{strerror(r)}: {prefix}")
+    return geno, pheno
+
+
+def perm_pvalue(observed, replicate_best):
+    """Permutation p-value: (1 + #{replicate best <= observed}) / (1 + replicates)."""
+    rb = np.ascontiguousarray(np.asarray(replicate_best, dtype=np.float32))
+    return float(library().epik2_perm_pvalue(np.float32(observed), _ptr(rb), len(rb)))
 
 
 def n_triplets(m):

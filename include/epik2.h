@@ -173,6 +173,23 @@ int epik2_scan(epik2_ctx *ctx, int32_t dataset_id, const epik2_opts *opts, epik2
  * ties by index) into out[0..K).  *n_out receives the number written. */
 int epik2_scan_topk(epik2_ctx *ctx, int32_t dataset_id, const epik2_opts *opts, epik2_best *out,
                     int32_t capacity, int32_t *n_out);
+/* --------------------------------------------------------------------------------
+ * Input files (no reference counterpart: the reference reads no files; its input is the
+ * synthetic generate_data, GPU/v4.cpp:81-110).  PLINK 1 binary fileset <prefix>.bed/.bim/.fam:
+ * the genotype is the count of the .bim's first allele (0, 1, 2); samples whose .fam
+ * phenotype (column 6) is neither 2 (case) nor 1 (control) are left out; a missing
+ * genotype takes `missing_genotype`.  epik2_plink_dims gives the sizes of the matrix that
+ * epik2_read_plink fills (sample-major n_samples x n_snps bytes, n_samples phenotypes).
+ * ------------------------------------------------------------------------------ */
+int epik2_plink_dims(const char *prefix, int64_t *n_samples, int64_t *n_snps);
+int epik2_read_plink(const char *prefix, uint8_t missing_genotype, uint8_t *geno, uint8_t *pheno);
+
+/* Permutation test (no reference counterpart): p-value of an observed best score against
+ * the best scores of phenotype-permutation replicates (epik2_load_replicate / the server's
+ * replicate requests): (1 + #{replicate best <= observed}) / (1 + n_replicates); lower K2
+ * is the stronger association.  -1 on invalid arguments. */
+double epik2_perm_pvalue(float observed, const float *replicate_best, int64_t n_replicates);
+
 /* One call from host buffers to the best triplet: load + scan + unload. */
 int epik2_scan_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int64_t n_samples,
                   int64_t n_snps, const epik2_opts *opts, epik2_best *out);
