@@ -606,14 +606,16 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       }
       tc_fence_before();
       __syncthreads();
-      // 32 pairs x 64 k of this half: triplet x = tid + 512u -> kl = x & 63, q = x >> 6
+      // 32 pairs x nk k of this half (nk = 64, or 48 in the FP4 tile's second half):
+      // triplet x = tid + 512u -> kl = x % nk, q = x / nk; every thread scores nk/16
+      const int nk = (64 * h + 64 <= kK) ? 64 : kK - 64 * h;
 #pragma unroll 1
-      for (int u = 0; u < (worker ? 4 : 0); u++) {
+      for (int u = 0; u < (worker ? nk / 16 : 0); u++) {
         const int x = tid + kTcThreads * u;
-        const int kl = x & 63, q = x >> 6;
+        const int q = x / nk, kl = x - q * nk;
         const int j = j0 + q;
         const int k = k0 + 64 * h + kl;
-        const bool valid = (64 * h + kl < kK) && (j < m) && (k > j) && (k < m);
+        const bool valid = (j < m) && (k > j) && (k < m);
         float sc = FLT_MAX;
         unsigned long long key = ~0ull;
         if (valid) {
