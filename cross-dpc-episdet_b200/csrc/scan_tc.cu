@@ -329,6 +329,8 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   float list_s = FLT_MAX;
   unsigned long long list_k = ~0ull;
   uint32_t g_chunk = 0, n_tile = 0, n_fetch = 0;
+  unsigned long long pf_t = 0;  // thread 0: ticket and descriptor of the next tile
+  long long pf_d = -1;
   const uint32_t* E = reinterpret_cast<const uint32_t*>(smem);  // epilogue staging, reuses the stages
 
   // Batched form: fold the CTA's candidates for dataset jb into its slot of that dataset.
@@ -371,11 +373,19 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
 
   for (;;) {
     // next tile from the shared queue; its descriptor (one 8-byte load) gives the dataset,
-    // the first index, the pair block and the k block
+    // the first index, the pair block and the k block.  Thread 0 takes the ticket and the
+    // descriptor of the tile after it right away, so their latency overlaps this tile.
     if (tid == 0) {
       if (issuer_cta) {
-        const unsigned long long t = atomicAdd(p.counter, 1ull);
-        const long long d = (t < (unsigned long long)p.n_tiles && !s_abort) ? (long long)__ldg(p.tiles + t) : -1ll;
+        if (n_fetch == 0) {
+          pf_t = atomicAdd(p.counter, 1ull);
+          pf_d = pf_t < (unsigned long long)p.n_tiles ? (long long)__ldg(p.tiles + pf_t) : -1ll;
+        }
+        const long long d = s_abort ? -1ll : pf_d;
+        if (d >= 0) {
+          pf_t = atomicAdd(p.counter, 1ull);
+          pf_d = pf_t < (unsigned long long)p.n_tiles ? (long long)__ldg(p.tiles + pf_t) : -1ll;
+        }
         s_tile = d;
         if (kPair) {  // hand the tile to the odd CTA: store, then release-arrive on its barrier
           st_cluster_s64(map_cta(smem_u32(&s_tile), 1), d);
