@@ -75,6 +75,19 @@ __device__ __forceinline__ float k2_score(const uint32_t (&T0)[27], const uint32
   return fabsf(score);
 }
 
+// The same sum with the table in shared memory (lut points into the kernel's dynamic
+// shared memory, so the lookups compile to shared-memory loads).
+__device__ __forceinline__ float k2_score_shared(const uint32_t (&T0)[27], const uint32_t (&T1)[27],
+                                                 const float* lut) {
+  float score = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 27; c++) {
+    const float d = __fsub_rn(lut[T0[c] + T1[c] + 1], lut[T0[c]]);
+    score = __fadd_rn(score, __fsub_rn(d, lut[T1[c]]));
+  }
+  return fabsf(score);
+}
+
 // Insert (s, key) into a warp-distributed sorted list (lane r holds the r-th best).
 __device__ __forceinline__ void warp_list_insert(float& ls, unsigned long long& lk, float s, unsigned long long key,
                                                  int lane) {

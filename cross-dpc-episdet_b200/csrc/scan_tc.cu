@@ -40,8 +40,15 @@ constexpr int kTcThreads = 512;  // 16 operand-producing / epilogue warps
 constexpr int kTcWarps = kTcThreads / 32;
 constexpr int kTcThreadsAll = kTcThreads + 32;  // + one warp that only issues the MMAs
 constexpr int kRingBytes = 16 * 384 * 32;  // stage ring: kStages x 384 rows x (32 * kW) bytes = 192 KiB
-constexpr int kTcSmemBytes = kRingBytes + 256;  // + mbarriers
+constexpr int kTcSmemBytes = 230400;        // ring (or epilogue staging + ln n! table), mbarriers at the end
+constexpr int kBarOff = kTcSmemBytes - 256;
 constexpr int kEStride = 129;  // words per row of the epilogue staging buffer
+// During a tile's epilogue the ring is idle: it holds the staging buffer E (2 classes x 128
+// rows x kEStride words) and, behind it, a copy of the dataset's ln n! table when the table
+// has at most kLutCapacity entries (samples + 2; larger tables are read from global memory).
+constexpr int kLutOff = 2 * 128 * kEStride * 4;
+constexpr int kLutCapacity = (kBarOff - kLutOff) / 4;
+static_assert(kRingBytes <= kBarOff && kLutOff % 16 == 0, "shared-memory layout");
 constexpr long long kWaitLimit = 4000000000LL;  // SM clocks (~2 s) before a wait gives up
 // instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = 256, M = 128
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
@@ -229,6 +236,11 @@ __device__ __forceinline__ uint4 expand32_fp4(uint32_t w) {
   return make_uint4(w & 0x11111111u, (w >> 1) & 0x11111111u, (w >> 2) & 0x11111111u, (w >> 3) & 0x11111111u);
 }
 
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void sts128(uint32_t saddr, uint4 v) {
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(saddr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
                : "memory");
@@ -272,7 +284,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   __shared__ int s_abort;
   __shared__ float s_red_s[kTcWarps];
   __shared__ unsigned long long s_red_k[kTcWarps];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kRingBytes);  // [stages] empty + acc
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBarOff);  // [stages] empty + acc
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t stage0 = smem_u32(smem);
   const uint32_t bar0 = smem_u32(bars);
@@ -586,6 +598,14 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     const int64_t tri = jv.tri;
     const uint2 si0 = *reinterpret_cast<const uint2*>(jv.singles + ((int64_t)i) * 2);
     const uint2 si1 = *reinterpret_cast<const uint2*>(jv.singles + (m_pad + i) * 2);
+    // ln n! table into the idle ring (in flight during the accumulator copy below); the
+    // device table is padded to 256 bytes, so whole 16-byte pieces stay inside it
+    const float* lut_s = reinterpret_cast<const float*>(smem + kLutOff);
+    const bool lut_shared = jv.n0 + jv.n1 + 2 <= kLutCapacity;
+    if (lut_shared && worker) {
+      const int n16 = (jv.n0 + jv.n1 + 2 + 3) / 4;
+      for (int x = tid; x < n16; x += kTcThreads) cp_async16(stage0 + kLutOff + 16 * x, jv.lut + 4 * x);
+    }
     for (int h = 0; h < 2; h++) {
       uint32_t* Ew = reinterpret_cast<uint32_t*>(smem);
 #pragma unroll
@@ -614,6 +634,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
           }
         }
       }
+      cp_async_wait_all();
       tc_fence_before();
       __syncthreads();
       // 32 pairs x nk k of this half (nk = 64, or 48 in the FP4 tile's second half):
@@ -648,7 +669,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
           uint32_t T0[27], T1[27];
           complete_table(t80, (uint32_t)jv.n0, si0, sj0, sk0, pij0, pik0, pjk0, T0);
           complete_table(t81, (uint32_t)jv.n1, si1, sj1, sk1, pij1, pik1, pjk1, T1);
-          sc = k2_score(T0, T1, jv.lut);
+          sc = lut_shared ? k2_score_shared(T0, T1, lut_s) : k2_score(T0, T1, jv.lut);
           key = pack_key((uint64_t)i, (uint64_t)j, (uint64_t)k);
           if (kDump) {
             const int64_t t = triplet_index(m, i, j, k);
