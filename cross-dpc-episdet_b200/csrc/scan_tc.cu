@@ -262,8 +262,10 @@ struct JobView {
 // that the scale factors fit in tensor memory beside the two accumulators, kW = 8 or 16:
 // 4 stages of 44 KiB or 2 of 88 KiB).  kW = class words (32 samples each) per stage.
 // kPair (FP4 only): a cluster of two CTAs computes one tile of 64 pairs (M = 256,
-// cta_group::2): CTA r holds the A rows of pairs j0+32r.. and the B rows of g_k = r, so each
-// CTA expands 128 + 112 operand rows per stage instead of 128 + 224; the even CTA issues.
+// cta_group::2): CTA r holds the A rows of pairs j0+32r.. and the B rows of SNPs
+// k0+56r..k0+56r+55 (both values of g_k), so each CTA expands 128 + 112 operand rows per
+// stage instead of 128 + 224; D column 112h + 56c + kp is SNP k0 + 56h + kp, g_k = c.
+// The even CTA issues.
 // kBatched: tiles of many datasets on one queue, per-dataset results.
 template <int kW, bool kFp4, bool kPair, bool kBatched, bool kDump, bool kTopK>
 __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) {
@@ -438,7 +440,8 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     //   A: pair q = lane, word wA = warp % kW: loads the i and j words once and writes rows
     //      32*ab + q (g_i = ab>>1, g_j = ab&1) for kAb = kW/4 consecutive ab
     //   B: words w = (tid>>7) + 4r (r < kU), kl = tid&127 (< kK) -> rows kK*c + kl (g_k = c)
-    //      of both c
+    //      of both c; CTA pairs: words w = (tid>>6) + 8r (r < kW/8), kp = tid&63 (< kK/2) ->
+    //      rows (kK/2)*c + kp for SNP k0 + (kK/2)*rank + kp (one 8-byte load gives both c)
     // A warp writes 32 consecutive rows of one 16-byte K group per store (conflict-free).
     // The words of stage cc+1 are loaded while stage cc is expanded.
     constexpr int kAb = kW / 4;
@@ -448,6 +451,12 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     const bool b_on = b_kl < kK;
     const int b_k = k0 + b_kl;
     const uint32_t offb0 = (b_kl >> 3) * kSbo + (b_kl & 7) * 16;  // + (kK/8)*kSbo for c = 1
+    // CTA pairs: B rows (kK/2)*c + kp of this CTA hold SNP k0 + (kK/2)*rank + kp, kp < kK/2
+    const int p_kl = tid & 63;
+    const bool p_on = p_kl < kK / 2;
+    const int p_k = k0 + (kK / 2) * (int)crank + p_kl;
+    const uint32_t offp0 = (p_kl >> 3) * kSbo + (p_kl & 7) * 16;  // + (kK/16)*kSbo for c = 1
+    const int p_wbase = tid >> 6;  // words p_wbase + 8r, r < kW/8
     auto load_words = [&](int cc, uint2& gi, uint2& gj, uint2 (&gk)[kU]) {
       const bool c1 = cc >= nc0;
       const int c_in = c1 ? cc - nc0 : cc;
@@ -461,14 +470,18 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         gj = __ldg(row + a_j);
       }
 #pragma unroll
-      for (int r = 0; r < kU; r++) {
-        const int w = w_base + 4 * r;
-        gk[r] = make_uint2(0, 0);
-        if (kW * c_in + w < wcls && b_on && b_k < m_pad) {
-          if (kPair)  // this CTA's B rows: g_k = rank only
-            gk[r].x = __ldg(reinterpret_cast<const uint32_t*>(jv.planes + (wb + w) * m_pad + b_k) + crank);
-          else
-            gk[r] = __ldg(jv.planes + (wb + w) * m_pad + b_k);
+      for (int r = 0; r < kU; r++) gk[r] = make_uint2(0, 0);
+      if (kPair) {
+#pragma unroll
+        for (int r = 0; r < kW / 8; r++) {
+          const int w = p_wbase + 8 * r;
+          if (kW * c_in + w < wcls && p_on && p_k < m_pad) gk[r] = __ldg(jv.planes + (wb + w) * m_pad + p_k);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < kU; r++) {
+          const int w = w_base + 4 * r;
+          if (kW * c_in + w < wcls && b_on && b_k < m_pad) gk[r] = __ldg(jv.planes + (wb + w) * m_pad + b_k);
         }
       }
     };
@@ -500,23 +513,33 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
             sts128(offa + (2 * wA) * 128 + 128, expand16(wa >> 16));
           }
         }
+        if (kPair) {
 #pragma unroll
-        for (int r = 0; r < kU; r++) {
-          const int w = w_base + 4 * r;
-          if (kPair) {
-            if (b_on) sts128(sB + offb0 + w * 128, expand32_fp4(ck[r].x));
-          } else if (kFp4) {
-            if (b_on) {
-              const uint32_t offb = sB + offb0 + w * 128;
+          for (int r = 0; r < kW / 8; r++) {
+            const int w = p_wbase + 8 * r;
+            if (p_on) {
+              const uint32_t offb = sB + offp0 + w * 128;
               sts128(offb, expand32_fp4(ck[r].x));
-              sts128(offb + (kK / 8) * kSbo, expand32_fp4(ck[r].y));
+              sts128(offb + (kK / 16) * kSbo, expand32_fp4(ck[r].y));
             }
-          } else {
-            const uint32_t offb = sB + offb0 + (2 * w) * 128;
-            sts128(offb, expand16(ck[r].x));
-            sts128(offb + 128, expand16(ck[r].x >> 16));
-            sts128(offb + (kK / 8) * kSbo, expand16(ck[r].y));
-            sts128(offb + (kK / 8) * kSbo + 128, expand16(ck[r].y >> 16));
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < kU; r++) {
+            const int w = w_base + 4 * r;
+            if (kFp4) {
+              if (b_on) {
+                const uint32_t offb = sB + offb0 + w * 128;
+                sts128(offb, expand32_fp4(ck[r].x));
+                sts128(offb + (kK / 8) * kSbo, expand32_fp4(ck[r].y));
+              }
+            } else {
+              const uint32_t offb = sB + offb0 + (2 * w) * 128;
+              sts128(offb, expand16(ck[r].x));
+              sts128(offb + 128, expand16(ck[r].x >> 16));
+              sts128(offb + (kK / 8) * kSbo, expand16(ck[r].y));
+              sts128(offb + (kK / 8) * kSbo + 128, expand16(ck[r].y >> 16));
+            }
           }
         }
         ci = ni;
@@ -608,8 +631,35 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     }
     for (int h = 0; h < 2; h++) {
       uint32_t* Ew = reinterpret_cast<uint32_t*>(smem);
+      if (kPair) {
+        // CTA pairs: columns 112h + 56c + kp (kp < 56) hold SNP k0 + 56h + kp, g_k = c; they
+        // go to E[cls][lane][56c + kp], 7 groups of 16 columns per class and lane quarter
 #pragma unroll
-      for (int cls = 0; cls < 2; cls++) {
+        for (int cls = 0; cls < 2; cls++) {
+          const bool has = (cls ? nc1 > 0 : nc0 > 0) && worker;
+#pragma unroll
+          for (int t = 0; t < 2; t++) {
+            const int u = cgrp + 4 * t;  // warp-uniform
+            if (u < 7 && worker) {
+              uint32_t v[16];
+              if (has) {
+                tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(cls * 256 + 112 * h + 16 * u), v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int t2 = 0; t2 < 16; t2++) v[t2] = __float2uint_rn(__uint_as_float(v[t2]));
+              } else {
+#pragma unroll
+                for (int t2 = 0; t2 < 16; t2++) v[t2] = 0;
+              }
+              uint32_t* dst = Ew + (cls * 128 + row) * kEStride + 16 * u;
+#pragma unroll
+              for (int t2 = 0; t2 < 16; t2++) dst[t2] = v[t2];
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int cls = 0; cls < (kPair ? 0 : 2); cls++) {  // single CTAs: columns kK*c + kl
         const bool has = (cls ? nc1 > 0 : nc0 > 0) && worker;
 #pragma unroll
         for (int part = 0; part < 2; part++) {
@@ -637,16 +687,18 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       cp_async_wait_all();
       tc_fence_before();
       __syncthreads();
-      // 32 pairs x nk k of this half (nk = 64, or 48 in the FP4 tile's second half):
-      // triplet x = tid + 512u -> kl = x % nk, q = x / nk; every thread scores nk/16
-      const int nk = (64 * h + 64 <= kK) ? 64 : kK - 64 * h;
+      // 32 pairs x nk k of this half (nk = 64, or 48 in the FP4 tile's second half; 56 in
+      // both halves of a CTA pair's tile): triplet x = tid + 512u -> kl = x % nk, q = x / nk
+      const int nk = kPair ? kK / 2 : ((64 * h + 64 <= kK) ? 64 : kK - 64 * h);
+      const int kbase = kPair ? (kK / 2) * h : 64 * h;
+      constexpr int kEc = kPair ? kK / 2 : 64;  // staging column of (c, kl): kEc * c + kl
 #pragma unroll 1
-      for (int u = 0; u < (worker ? nk / 16 : 0); u++) {
+      for (int u = 0; u < (worker ? (32 * nk + kTcThreads - 1) / kTcThreads : 0); u++) {
         const int x = tid + kTcThreads * u;
         const int q = x / nk, kl = x - q * nk;
         const int j = j0 + q;
-        const int k = k0 + 64 * h + kl;
-        const bool valid = (j < m) && (k > j) && (k < m);
+        const int k = k0 + kbase + kl;
+        const bool valid = (q < 32) && (j < m) && (k > j) && (k < m);
         float sc = FLT_MAX;
         unsigned long long key = ~0ull;
         if (valid) {
@@ -655,8 +707,8 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
           for (int ab = 0; ab < 4; ab++)
 #pragma unroll
             for (int c = 0; c < 2; c++) {
-              t80[2 * ab + c] = E[(0 * 128 + 32 * ab + q) * kEStride + 64 * c + kl];
-              t81[2 * ab + c] = E[(1 * 128 + 32 * ab + q) * kEStride + 64 * c + kl];
+              t80[2 * ab + c] = E[(0 * 128 + 32 * ab + q) * kEStride + kEc * c + kl];
+              t81[2 * ab + c] = E[(1 * 128 + 32 * ab + q) * kEStride + kEc * c + kl];
             }
           const uint2 sj0 = *reinterpret_cast<const uint2*>(jv.singles + ((int64_t)j) * 2);
           const uint2 sj1 = *reinterpret_cast<const uint2*>(jv.singles + (m_pad + j) * 2);
