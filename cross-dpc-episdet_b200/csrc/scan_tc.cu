@@ -42,7 +42,7 @@ constexpr int kTcThreadsAll = kTcThreads + 32;  // + one warp that only issues t
 constexpr int kRingBytes = 16 * 384 * 32;  // stage ring: kStages x 384 rows x (32 * kW) bytes = 192 KiB
 constexpr int kTcSmemBytes = 230400;        // ring (or epilogue staging + ln n! table), mbarriers at the end
 constexpr int kBarOff = kTcSmemBytes - 256;
-constexpr int kEStride = 129;  // words per row of the epilogue staging buffer
+constexpr int kEStride = 132;  // words per row of the epilogue staging buffer (16-byte rows: 128-bit stores)
 // During a tile's epilogue the ring is idle: it holds the staging buffer E (2 classes x 128
 // rows x kEStride words) and, behind it, a copy of the dataset's ln n! table when the table
 // has at most kLutCapacity entries (samples + 2; larger tables are read from global memory).
@@ -279,6 +279,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   constexpr uint32_t kSbo = 8 * kRowBytes;            // bytes between 8-row groups
   constexpr int kMmas = kFp4 ? kW / 2 : kW;           // MMAs per stage (K = 64 E2M1 or 32 int8)
   constexpr int kU = kW / 4;                          // units of each kind per thread per stage
+  constexpr int kUB = kPair ? kW / 8 : kU;            // 8-byte B plane loads per thread per stage
   static_assert(kStages >= 2 && kStages <= 4, "stage ring");
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t s_tmem;
@@ -457,7 +458,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     const int p_k = k0 + (kK / 2) * (int)crank + p_kl;
     const uint32_t offp0 = (p_kl >> 3) * kSbo + (p_kl & 7) * 16;  // + (kK/16)*kSbo for c = 1
     const int p_wbase = tid >> 6;  // words p_wbase + 8r, r < kW/8
-    auto load_words = [&](int cc, uint2& gi, uint2& gj, uint2 (&gk)[kU]) {
+    auto load_words = [&](int cc, uint2& gi, uint2& gj, uint2 (&gk)[kUB]) {
       const bool c1 = cc >= nc0;
       const int c_in = c1 ? cc - nc0 : cc;
       const int wcls = c1 ? jv.w1 : jv.w0;
@@ -470,8 +471,8 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         gj = __ldg(row + a_j);
       }
 #pragma unroll
-      for (int r = 0; r < kU; r++) gk[r] = make_uint2(0, 0);
-      if (kPair) {
+      for (int r = 0; r < kUB; r++) gk[r] = make_uint2(0, 0);
+      if constexpr (kPair) {
 #pragma unroll
         for (int r = 0; r < kW / 8; r++) {
           const int w = p_wbase + 8 * r;
@@ -486,13 +487,13 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       }
     };
     if (worker) {
-      uint2 ci, cj, ck[kU];
+      uint2 ci, cj, ck[kUB];
       if (nct > 0) load_words(0, ci, cj, ck);
       for (int cc = 0; cc < nct; ++cc) {
         const uint32_t g = g_chunk + (uint32_t)cc;
-        uint2 ni = make_uint2(0, 0), nj = ni, nk[kU];
+        uint2 ni = make_uint2(0, 0), nj = ni, nk[kUB];
 #pragma unroll
-        for (int r = 0; r < kU; r++) nk[r] = make_uint2(0, 0);
+        for (int r = 0; r < kUB; r++) nk[r] = make_uint2(0, 0);
         if (cc + 1 < nct) load_words(cc + 1, ni, nj, nk);
         const int s = (int)(g % kStages);
         const uint32_t use = g / kStages;
@@ -513,7 +514,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
             sts128(offa + (2 * wA) * 128 + 128, expand16(wa >> 16));
           }
         }
-        if (kPair) {
+        if constexpr (kPair) {
 #pragma unroll
           for (int r = 0; r < kW / 8; r++) {
             const int w = p_wbase + 8 * r;
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         ci = ni;
         cj = nj;
 #pragma unroll
-        for (int r = 0; r < kU; r++) ck[r] = nk[r];
+        for (int r = 0; r < kUB; r++) ck[r] = nk[r];
         fence_proxy_async();
         __syncwarp();
         if (lane == 0) bar_arrive(bar_full0 + 8 * s);
@@ -630,7 +631,6 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       for (int x = tid; x < n16; x += kTcThreads) cp_async16(stage0 + kLutOff + 16 * x, jv.lut + 4 * x);
     }
     for (int h = 0; h < 2; h++) {
-      uint32_t* Ew = reinterpret_cast<uint32_t*>(smem);
       if (kPair) {
         // CTA pairs: columns 112h + 56c + kp (kp < 56) hold SNP k0 + 56h + kp, g_k = c; they
         // go to E[cls][lane][56c + kp], 7 groups of 16 columns per class and lane quarter
@@ -651,9 +651,9 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
 #pragma unroll
                 for (int t2 = 0; t2 < 16; t2++) v[t2] = 0;
               }
-              uint32_t* dst = Ew + (cls * 128 + row) * kEStride + 16 * u;
+              const uint32_t dst = stage0 + 4 * ((cls * 128 + row) * kEStride + 16 * u);
 #pragma unroll
-              for (int t2 = 0; t2 < 16; t2++) dst[t2] = v[t2];
+              for (int t2 = 0; t2 < 4; t2++) sts128(dst + 16 * t2, make_uint4(v[4 * t2], v[4 * t2 + 1], v[4 * t2 + 2], v[4 * t2 + 3]));
             }
           }
         }
@@ -677,10 +677,10 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
 #pragma unroll
             for (int t = 0; t < 16; t++) v[t] = 0;
           }
-          uint32_t* dst = Ew + (cls * 128 + row) * kEStride + 64 * e_c + 32 * e_sub + 16 * part;
+          const uint32_t dst = stage0 + 4 * ((cls * 128 + row) * kEStride + 64 * e_c + 32 * e_sub + 16 * part);
           if (worker) {
 #pragma unroll
-            for (int t = 0; t < 16; t++) dst[t] = v[t];
+            for (int t = 0; t < 4; t++) sts128(dst + 16 * t, make_uint4(v[4 * t], v[4 * t + 1], v[4 * t + 2], v[4 * t + 3]));
           }
         }
       }
