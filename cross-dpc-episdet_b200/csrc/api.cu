@@ -25,6 +25,10 @@ struct epik2_ctx {
   std::string last_error;
   std::map<int32_t, std::unique_ptr<DevDataset>> datasets;
   int32_t next_id = 1;
+  // one dataset allocation kept by the one-call entry point (epik2_scan_u8) for its next
+  // call: allocating and freeing a few hundred MiB per call costs tens to hundreds of ms
+  void* spare_block = nullptr;
+  size_t spare_bytes = 0;
   // search scratch
   int engine = 0;               // default engine: 0 = auto, 1 = integer, 2 = tensor cores int8, 3 = tensor cores FP4
   int stage_words = 0;          // default tensor-core stage depth: 0 = autotuned
@@ -114,6 +118,27 @@ int cuda_fail(epik2_ctx* ctx, cudaError_t e, const char* what) {
   } while (0)
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+void drop_spare(epik2_ctx* ctx) {
+  if (ctx->spare_block) cudaFree(ctx->spare_block);
+  ctx->spare_block = nullptr;
+  ctx->spare_bytes = 0;
+}
+
+// A dataset allocation of at least `bytes`: the context's spare block when it fits without
+// more than doubling the footprint, else a new one (the spare is released first).
+cudaError_t take_block(epik2_ctx* ctx, size_t bytes, void** out, size_t* got) {
+  if (ctx->spare_block && ctx->spare_bytes >= bytes && ctx->spare_bytes <= 2 * bytes) {
+    *out = ctx->spare_block;
+    *got = ctx->spare_bytes;
+    ctx->spare_block = nullptr;
+    ctx->spare_bytes = 0;
+    return cudaSuccess;
+  }
+  drop_spare(ctx);
+  *got = bytes;
+  return cudaMalloc(out, bytes);
+}
 
 struct Layout {
   size_t geno, perm, planes, singles, pairs, lut, lut64, total;
@@ -806,6 +831,7 @@ void epik2_destroy(epik2_ctx* ctx) {
   ctx->plans.clear();
   for (auto& kv : ctx->datasets) cudaFree(kv.second->block);
   ctx->datasets.clear();
+  cudaFree(ctx->spare_block);
   cudaFree(ctx->d_counter);
   cudaFree(ctx->d_slots);
   cudaFree(ctx->d_best);
@@ -913,9 +939,10 @@ int epik2_load_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int
   const Layout L = dataset_layout(n_samples, n_snps);
   size_t fr = 0, tot = 0;
   CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
-  if (L.total + (size_t)(256u << 20) > fr) return fail(ctx, EPIK2_E_NOMEM, "dataset does not fit in free device memory");
+  if (L.total + (size_t)(256u << 20) > fr + ctx->spare_bytes)
+    return fail(ctx, EPIK2_E_NOMEM, "dataset does not fit in free device memory");
   std::unique_ptr<DevDataset> d(new DevDataset());
-  CK(ctx, cudaMalloc(&d->block, L.total), "alloc dataset");
+  CK(ctx, take_block(ctx, L.total, &d->block, &d->block_bytes), "alloc dataset");
   char* b = (char*)d->block;
   d->bytes = L.total;
   d->n_samples = n_samples;
@@ -982,7 +1009,7 @@ int epik2_load_replicate(epik2_ctx* ctx, int32_t base_dataset_id, const uint8_t*
   CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
   if (L.total + (size_t)(256u << 20) > fr) return fail(ctx, EPIK2_E_NOMEM, "replicate does not fit in free device memory");
   std::unique_ptr<DevDataset> d(new DevDataset());
-  CK(ctx, cudaMalloc(&d->block, L.total), "alloc replicate");
+  CK(ctx, take_block(ctx, L.total, &d->block, &d->block_bytes), "alloc replicate");
   char* b = (char*)d->block;
   d->bytes = L.total;
   d->n_samples = root->n_samples;
@@ -1018,7 +1045,9 @@ int epik2_load_replicate(epik2_ctx* ctx, int32_t base_dataset_id, const uint8_t*
   return EPIK2_OK;
 }
 
-int epik2_unload(epik2_ctx* ctx, int32_t dataset_id) {
+namespace {
+// keep: the allocation becomes the context's spare block (the one-call entry point)
+int unload_dataset(epik2_ctx* ctx, int32_t dataset_id, bool keep) {
   if (!ctx) return EPIK2_E_INVALID;
   auto it = ctx->datasets.find(dataset_id);
   if (it == ctx->datasets.end()) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
@@ -1029,10 +1058,19 @@ int epik2_unload(epik2_ctx* ctx, int32_t dataset_id) {
   }
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  cudaFree(it->second->block);
+  if (keep) {
+    drop_spare(ctx);
+    ctx->spare_block = it->second->block;
+    ctx->spare_bytes = it->second->block_bytes;
+  } else {
+    cudaFree(it->second->block);
+  }
   ctx->datasets.erase(it);
   return EPIK2_OK;
 }
+}  // namespace
+
+int epik2_unload(epik2_ctx* ctx, int32_t dataset_id) { return unload_dataset(ctx, dataset_id, false); }
 
 int epik2_dataset_info(const epik2_ctx* ctx, int32_t dataset_id, int64_t* n_samples, int64_t* n_snps,
                        int64_t* n_cases, int64_t* device_bytes) {
@@ -1094,7 +1132,7 @@ int epik2_scan_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int
   int r = epik2_load_u8(ctx, geno, pheno, n_samples, n_snps, &id);
   if (r) return r;
   r = epik2_scan(ctx, id, opts, out);
-  epik2_unload(ctx, id);
+  unload_dataset(ctx, id, true);
   return r;
 }
 

@@ -27,7 +27,8 @@ struct DevDataset {
   double* lut64 = nullptr;      // ln n! in double (precision form), [0, n_samples+1]
   int64_t tri = 0;              // entries per class in `pairs`
   void* block = nullptr;        // single allocation holding all of the above
-  size_t bytes = 0;
+  size_t bytes = 0;             // bytes the layout needs
+  size_t block_bytes = 0;       // size of `block` (at least `bytes`)
   int32_t base_id = -1;         // replicate: dataset whose genotype matrix this one shares
   int32_t n_replicates = 0;     // live replicates sharing this dataset's genotypes
 };

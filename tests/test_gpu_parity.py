@@ -81,6 +81,18 @@ def test_ragged_shapes_vs_oracle(ctx, seed, S, M, cases):
         ctx.unload(did)
 
 
+def test_one_call_entry_point_reuses_its_allocation(ctx):
+    """epik2_scan_u8 keeps one dataset allocation for its next call; nothing of the previous
+    dataset may show through (same shape, smaller within 2x, much smaller, larger)."""
+    for seed, S, M, cases in [(51, 2000, 80, 1000), (52, 2000, 80, 700), (53, 1900, 76, 1000), (54, 64, 10, 30),
+                              (55, 2100, 84, 1050)]:
+        g, p = O.gen_hwe(seed, S, M, cases)
+        r = O.scan(g, p)
+        b = ctx.scan_u8(g, p)
+        assert b.ijk == r["ijk"]
+        assert f32_bits(b.score) == f32_bits(r["score"])
+
+
 def test_planted_ties_break_to_lowest_index(ctx):
     # Duplicate SNP columns make many triplets share an exact score.
     g, p = O.gen_hwe(50, 500, 12, 250)
