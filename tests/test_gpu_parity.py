@@ -81,6 +81,24 @@ def test_ragged_shapes_vs_oracle(ctx, seed, S, M, cases):
         ctx.unload(did)
 
 
+@pytest.mark.parametrize("seed,S,M", [(61, 23742, 40), (62, 23743, 36), (63, 40000, 40)])
+def test_large_sample_counts_vs_oracle(ctx, seed, S, M):
+    """Up to 23,742 samples the tensor-core epilogue reads the ln n! table from a shared-memory
+    copy, beyond it from global memory: both sides of that limit, tables included."""
+    g, p = O.gen_hwe(seed, S, M, S // 2)
+    r = O.scan(g, p, with_tables=True)
+    did = ctx.load(g, p)
+    try:
+        b = ctx.scan(did)
+        assert b.ijk == r["ijk"]
+        assert f32_bits(b.score) == f32_bits(r["score"])
+        tables, scores = ctx.dump_tables(did)
+        assert np.array_equal(tables, r["tables"])
+        assert np.array_equal(scores.view(np.uint32), r["scores"].view(np.uint32))
+    finally:
+        ctx.unload(did)
+
+
 def test_one_call_entry_point_reuses_its_allocation(ctx):
     """epik2_scan_u8 keeps one dataset allocation for its next call; nothing of the previous
     dataset may show through (same shape, smaller within 2x, much smaller, larger)."""
