@@ -1,30 +1,33 @@
-// Tensor-core engine of the triplet search (tcgen05, kind::i8, sm_100a).
+// Tensor-core engine of the triplet search (tcgen05, sm_100a): kind::i8 and block-scaled
+// kind::mxf4 (FP4), single CTAs or CTA pairs (cta_group::2).
 //
 // Same result as the integer engine (scan_int.cu) and as the reference's kernel_epi
 // (GPU/v4.cpp:295-594): the 8 cells of each triplet with g_i, g_j, g_k in {0,1} are
 // counted exactly, the other 19 per class follow by inclusion-exclusion, K2 is scored in
 // the reference's FP32 order, and the lowest (score, i, j, k) wins.
 //
-// Counting as an integer matrix product.  For a fixed SNP i, a block of 32 SNPs j and a
-// block of 128 SNPs k, with 0/1 indicators x_{s,g}(snp) = [genotype of snp in sample s
-// is g]:
+// Counting as a matrix product.  For a fixed SNP i, a block of 32 SNPs j and a block of kK
+// SNPs k (128 in the int8 format, 112 in FP4), with 0/1 indicators x_{s,g}(snp) =
+// [genotype of snp in sample s is g]:
 //     D[(j, a, b)][(k, c)] = sum over samples s of class C of
 //                            x_{s,a}(i) * x_{s,b}(j)  *  x_{s,c}(k)
 //                          = count of (g_i=a, g_j=b, g_k=c) in class C.
-// A (128 x S_C) holds the pair indicators of the 32 pairs (i, j) x (a, b), B (256 x S_C)
-// the single indicators of the 128 SNPs k x c; both are expanded from the bit planes to
-// int8 (0 or -1), 32*kW samples per pipeline stage, straight into shared memory in the
-// no-swizzle K-major layout the tensor core reads (8-row x 16-byte core matrices;
-// K-neighbours 128 B apart).  Warp roles: 16 warps expand operands (and later run the
-// epilogue); one more warp only issues tcgen05.mma (M=128, N=256, K=32, int32 accumulators
-// in tensor memory: class 0 into TMEM columns [0,256), class 1 into [256,512)).  An MMA
-// issue blocks its thread for about the MMA's execution time, so the issuing thread does
-// nothing else.  Hand-off per stage: each producing warp fences its stores for the async
-// proxy and arrives once on the stage's "full" mbarrier; the issuer waits on it, issues
-// the stage's MMAs and commits them to the stage's "empty" mbarrier, which the producers
-// wait on before refilling the slot (and, at the end of a tile, to the accumulator
-// barrier).  The epilogue moves the accumulators TMEM -> registers -> shared memory and
-// completes, scores and selects the 32 x 128 triplets of the tile.
+// A (128 x S_C) holds the pair indicators of the 32 pairs (i, j) x (a, b), B (2kK x S_C)
+// the single indicators of the kK SNPs k x c; both are expanded from the bit planes (int8
+// 0 or -1; E2M1 0 or 0.5 with scale factors 2), 32*kW samples per pipeline stage, straight
+// into shared memory in the no-swizzle K-major layout the tensor core reads (8-row x
+// 16-byte core matrices; K-neighbours 128 B apart).  Warp roles: 16 warps expand operands
+// (and later run the epilogue); one more warp only issues tcgen05.mma (int8: M=128, N=256,
+// K=32, int32 accumulators; FP4: N=224, K=64, FP32 accumulators exact below 2^24; class 0
+// and class 1 into separate halves of tensor memory).  An MMA issue blocks its thread for
+// about the MMA's execution time, so the issuing thread does nothing else.  Hand-off per
+// stage: each producing warp fences its stores for the async proxy and arrives once on the
+// stage's "full" mbarrier; the issuer waits on it, issues the stage's MMAs and commits them
+// to the stage's "empty" mbarrier, which the producers wait on before refilling the slot
+// (and, at the end of a tile, to the accumulator barrier).  CTA pairs compute 64 pairs j at
+// once (M=256), each CTA expanding half of A and half of B.  The epilogue moves the
+// accumulators TMEM -> registers -> shared memory and completes, scores and selects the
+// triplets of the tile, with the ln n! table copied into the then idle stage ring.
 //
 // Every wait on an mbarrier is bounded (about 2 s of SM clock); on expiry the kernel sets
 // an error word, stops taking tiles, frees its tensor memory and returns.
