@@ -190,7 +190,9 @@ int epik2_read_plink(const char *prefix, uint8_t missing_genotype, uint8_t *geno
  * is the stronger association.  -1 on invalid arguments. */
 double epik2_perm_pvalue(float observed, const float *replicate_best, int64_t n_replicates);
 
-/* One call from host buffers to the best triplet: load + scan + unload. */
+/* One call from host buffers to the best triplet: load + scan + unload.  The context keeps
+ * the dataset's device allocation for its next load (reused when it fits within twice the
+ * size, else released first); epik2_destroy releases it. */
 int epik2_scan_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int64_t n_samples,
                   int64_t n_snps, const epik2_opts *opts, epik2_best *out);
 
