@@ -91,3 +91,16 @@ def test_cli_usage_errors():
         pytest.skip("CLI not built")
     r = subprocess.run([epik2.CLI_PATH], capture_output=True, text=True)
     assert r.returncode == 2 and "usage" in r.stderr
+
+
+def test_cli_file_input_errors(tmp_path):
+    """Reading the --file matrix fails before any device is touched."""
+    if not os.path.exists(epik2.CLI_PATH):
+        pytest.skip("CLI not built")
+    path = tmp_path / "short.bin"
+    path.write_bytes(bytes(100))
+    r = subprocess.run([epik2.CLI_PATH, "--file", str(path), "50", "10"], capture_output=True, text=True)
+    assert r.returncode != 0 and "short read" in r.stderr
+    r = subprocess.run([epik2.CLI_PATH, "--file", str(tmp_path / "absent.bin"), "50", "10"], capture_output=True,
+                       text=True)
+    assert r.returncode != 0 and "cannot open" in r.stderr
