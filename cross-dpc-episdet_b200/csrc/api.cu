@@ -180,6 +180,9 @@ int64_t make_perm(const uint8_t* pheno, int64_t s, std::vector<int32_t>& perm) {
   return n1;
 }
 
+int run_pairs_tc(epik2_ctx* ctx, DevDataset& d);
+bool fp4_exact(const DevDataset& d);
+
 int encode_with(epik2_ctx* ctx, DevDataset& d, const uint8_t* pheno) {
   std::vector<int32_t> perm;
   d.n_cases = make_perm(pheno, d.n_samples, perm);
@@ -189,8 +192,12 @@ int encode_with(epik2_ctx* ctx, DevDataset& d, const uint8_t* pheno) {
   CK(ctx, cudaMemcpyAsync(d.perm, perm.data(), perm.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "upload perm");
   ctx->stats.h2d_bytes += perm.size() * 4;
   CK(ctx, launch_encode(d, ctx->stream), "encode kernel");
-  CK(ctx, launch_counts(d, ctx->stream), "count kernels");
-  ctx->stats.kernel_launches += 3;
+  // pair margins on tensor cores when FP4 counts are exact (classes below 2^24 samples),
+  // else on the integer pipe
+  const bool tc_pairs = fp4_exact(d) && d.m_pad >= 2;
+  CK(ctx, launch_counts(d, ctx->stream, !tc_pairs), "count kernels");
+  ctx->stats.kernel_launches += tc_pairs ? 2 : 3;
+  if (tc_pairs) return run_pairs_tc(ctx, d);
   CK(ctx, cudaStreamSynchronize(ctx->stream), "encode");
   return EPIK2_OK;
 }
@@ -400,6 +407,59 @@ int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_
       ctx->last_topk.push_back(e);
     }
   }
+  return EPIK2_OK;
+}
+
+// Pair margins on tensor cores: the CTA-pair FP4 kernel in its pair-margin form over pair
+// blocks (0, j0), j0 = 0, 64, ..., each with the k blocks of 112 SNPs from (j0 + 1) / 112
+// on; every (j, k), j < k < m_pad, is written once.  Waits for the result (stream sync).
+int run_pairs_tc(epik2_ctx* ctx, DevDataset& d) {
+  const int64_t m_pad = d.m_pad, kk = tc_k_per_tile(true);
+  const int64_t n_kb = (m_pad + kk - 1) / kk;
+  std::vector<uint32_t> ij;
+  std::vector<int64_t> off(1, 0);
+  for (int64_t j0 = 0; j0 <= m_pad - 2; j0 += 64) {
+    ij.push_back(0);
+    ij.push_back((uint32_t)j0);
+    off.push_back(off.back() + (n_kb - (j0 + 1) / kk));
+  }
+  const int64_t n_pb = (int64_t)off.size() - 1;
+  int r = ensure_pb(ctx, std::max<int64_t>(n_pb, 1));
+  if (r) return r;
+  r = ensure_tiles(ctx, std::max<int64_t>(off.back(), 1));
+  if (r) return r;
+  CK(ctx, cudaMemcpyAsync(ctx->d_pb_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, ctx->stream),
+     "upload pair-margin tiles");
+  CK(ctx, cudaMemcpyAsync(ctx->d_pb_ij, ij.data(), ij.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
+     "upload pair-margin tiles");
+  CK(ctx, launch_expand_tiles(ctx->d_pb_off, ctx->d_pb_ij, n_pb, true, 0, ctx->d_tiles, ctx->stream),
+     "expand pair-margin tiles");
+  CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream), "reset counter");
+  CK(ctx, cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream), "reset error word");
+  TcParams p{};
+  p.planes = d.planes;
+  p.singles = d.singles;
+  p.pairs = d.pairs;
+  p.lut = d.lut;
+  p.tiles = ctx->d_tiles;
+  p.n_tiles = off.back();
+  p.tri = d.tri;
+  p.m = (int32_t)d.n_snps;
+  p.m_pad = (int32_t)d.m_pad;
+  p.w0 = (int32_t)d.w0;
+  p.w1 = (int32_t)d.w1;
+  p.n0 = (int32_t)d.n_controls;
+  p.n1 = (int32_t)d.n_cases;
+  p.counter = ctx->d_counter;
+  p.slots = ctx->d_slots;
+  p.err = ctx->d_err;
+  p.pairs_out = d.pairs;
+  CK(ctx, launch_pairs_tc(p, tc_pair_blocks(ctx->tc_blocks), ctx->stream), "pair-margin kernel");
+  ctx->stats.kernel_launches += 2;
+  int err_word = 0;
+  CK(ctx, cudaMemcpyAsync(&err_word, ctx->d_err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read error word");
+  CK(ctx, cudaStreamSynchronize(ctx->stream), "encode");
+  if (err_word) return fail(ctx, EPIK2_E_TIMEOUT, "pair margins: a bounded wait expired");
   return EPIK2_OK;
 }
 

@@ -97,12 +97,12 @@ cudaError_t launch_encode(const DevDataset& d, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_counts(const DevDataset& d, cudaStream_t stream) {
+cudaError_t launch_counts(const DevDataset& d, cudaStream_t stream, bool pairs) {
   if (d.m_pad == 0) return cudaSuccess;
   k_singles<<<(unsigned)((d.m_pad + 255) / 256), 256, 0, stream>>>(d.planes, d.singles, d.m_pad, d.w0, d.w1);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  if (d.m_pad < 2) return cudaSuccess;
+  if (d.m_pad < 2 || !pairs) return cudaSuccess;
   dim3 grid((unsigned)d.m_pad, (unsigned)((d.m_pad + 255) / 256));
   k_pairs<<<grid, 256, 0, stream>>>(d.planes, d.pairs, d.m_pad, d.w0, d.w1);
   return cudaGetLastError();

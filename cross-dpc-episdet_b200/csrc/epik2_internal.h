@@ -122,11 +122,16 @@ struct TcParams {
   const TcJob* jobs;
   int32_t n_jobs;
   BestSlot* job_slots;     // [n_jobs][grid]
+  // pair-margin form (pairs_out != null): tiles (0, j0, k block) write the (j, k) pair
+  // counts of both classes instead of scoring triplets
+  uint4* pairs_out;
 };
 
 // Kernel launchers (scan_int.cu / scan_tc.cu / encode.cu); all asynchronous on `stream`.
 cudaError_t launch_encode(const DevDataset& d, cudaStream_t stream);
-cudaError_t launch_counts(const DevDataset& d, cudaStream_t stream);
+cudaError_t launch_counts(const DevDataset& d, cudaStream_t stream, bool pairs = true);
+// pair margins on tensor cores (the CTA-pair FP4 kernel; exact for classes below 2^24)
+cudaError_t launch_pairs_tc(const TcParams& p, int blocks, cudaStream_t stream);
 cudaError_t launch_scan_int(const ScanParams& p, int blocks, bool dump, cudaStream_t stream);
 cudaError_t launch_reduce_best(const BestSlot* slots, int n, BestSlot* out, cudaStream_t stream);
 cudaError_t launch_tables(const DevDataset& d, const uint32_t* triplets, int64_t n, uint32_t* out,

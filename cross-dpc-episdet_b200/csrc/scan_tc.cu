@@ -270,9 +270,13 @@ struct JobView {
 // stage instead of 128 + 224; D column 112h + 56c + kp is SNP k0 + 56h + kp, g_k = c.
 // The even CTA issues.
 // kBatched: tiles of many datasets on one queue, per-dataset results.
-template <int kW, bool kFp4, bool kPair, bool kBatched, bool kDump, bool kTopK>
+// kMarg (CTA pairs only): the pair-margin form.  Operand A's g_i = 0 rows are all ones and
+// its g_i = 1 rows zero, so D[(j, 0, b)][(k, c)] is the count of (g_j = b, g_k = c): tiles
+// (0, j0, k block) write the pair margins of every j < k < m_pad instead of scoring.
+template <int kW, bool kFp4, bool kPair, bool kBatched, bool kDump, bool kTopK, bool kMarg = false>
 __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) {
   static_assert(!kPair || kFp4, "CTA pairs use the FP4 format");
+  static_assert(!kMarg || (kPair && !kBatched && !kDump && !kTopK), "pair margins: plain CTA-pair kernel");
   constexpr int kK = kFp4 ? 112 : 128;                // SNPs k per tile -> 2*kK rows of B
   constexpr int kRowBytes = (kFp4 ? 16 : 32) * kW;    // operand bytes per row per stage
   constexpr int kBRows = kPair ? kK : 2 * kK;         // B rows held by this CTA
@@ -470,7 +474,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       gj = gi;
       if (kW * c_in + wA < wcls) {
         const uint2* row = jv.planes + (wb + wA) * m_pad;
-        gi = __ldg(row + i);
+        gi = kMarg ? make_uint2(~0u, 0u) : __ldg(row + i);
         gj = __ldg(row + a_j);
       }
 #pragma unroll
@@ -629,7 +633,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     // device table is padded to 256 bytes, so whole 16-byte pieces stay inside it
     const float* lut_s = reinterpret_cast<const float*>(smem + kLutOff);
     const bool lut_shared = jv.n0 + jv.n1 + 2 <= kLutCapacity;
-    if (lut_shared && worker) {
+    if (!kMarg && lut_shared && worker) {
       const int n16 = (jv.n0 + jv.n1 + 2 + 3) / 4;
       for (int x = tid; x < n16; x += kTcThreads) cp_async16(stage0 + kLutOff + 16 * x, jv.lut + 4 * x);
     }
@@ -695,8 +699,25 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       const int nk = kPair ? kK / 2 : ((64 * h + 64 <= kK) ? 64 : kK - 64 * h);
       const int kbase = kPair ? (kK / 2) * h : 64 * h;
       constexpr int kEc = kPair ? kK / 2 : 64;  // staging column of (c, kl): kEc * c + kl
+      if constexpr (kMarg) {
+        // pair margins (n00, n01, n10, n11) of (j, k): staging rows ab = g_j (g_i = 0), c = g_k
 #pragma unroll 1
-      for (int u = 0; u < (worker ? (32 * nk + kTcThreads - 1) / kTcThreads : 0); u++) {
+        for (int u = 0; u < (worker ? (32 * nk + kTcThreads - 1) / kTcThreads : 0); u++) {
+          const int x = tid + kTcThreads * u;
+          const int q = x / nk, kl = x - q * nk;
+          const int j = j0 + q, k = k0 + kbase + kl;
+          if (q < 32 && j < k && k < m_pad) {
+            const int64_t o = tri_offset(m_pad, j, k);
+#pragma unroll
+            for (int cls = 0; cls < 2; cls++) {
+              const uint32_t* Er = E + (cls * 128 + q) * kEStride + kl;
+              p.pairs_out[cls * tri + o] = make_uint4(Er[0], Er[kEc], Er[32 * kEStride], Er[32 * kEStride + kEc]);
+            }
+          }
+        }
+      }
+#pragma unroll 1
+      for (int u = 0; u < (worker && !kMarg ? (32 * nk + kTcThreads - 1) / kTcThreads : 0); u++) {
         const int x = tid + kTcThreads * u;
         const int q = x / nk, kl = x - q * nk;
         const int j = j0 + q;
@@ -894,6 +915,9 @@ cudaError_t tc_configure() {
     if (e == cudaSuccess) e = set_smem_all<8, false, false>();
     if (e == cudaSuccess) e = set_smem_all<8, true, false>();
     if (e == cudaSuccess) e = set_smem_all<16, true, true>();
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_scan_tc<16, true, true, false, false, false, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
     if (e != cudaSuccess) return e;
     configured = true;
   }
@@ -909,7 +933,7 @@ static void launch_variant(const TcParams& p, int blocks, bool batched, bool dum
 }
 
 // CTA-pair kernels: clusters of two CTAs
-template <bool kB, bool kD, bool kT>
+template <bool kB, bool kD, bool kT, bool kM = false>
 static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t stream) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)blocks);
@@ -923,7 +947,7 @@ static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t strea
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_scan_tc<16, true, true, kB, kD, kT>, p);
+  return cudaLaunchKernelEx(&cfg, k_scan_tc<16, true, true, kB, kD, kT, kM>, p);
 }
 
 int tc_k_per_tile(bool fp4) { return fp4 ? 112 : 128; }
@@ -978,6 +1002,13 @@ cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, b
     else launch_variant<4, false>(p, blocks, batched, dump, topk, stream);
   }
   return cudaGetLastError();
+}
+
+cudaError_t launch_pairs_tc(const TcParams& p, int blocks, cudaStream_t stream) {
+  const cudaError_t ce = tc_configure();
+  if (ce != cudaSuccess) return ce;
+  const cudaError_t e = launch_pair<false, false, false, true>(p, blocks & ~1, stream);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_reduce_jobs(const BestSlot* slots, int n_jobs, int per_job, BestSlot* out, cudaStream_t stream) {
