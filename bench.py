@@ -102,11 +102,16 @@ class ClockSampler:
                 "power_w_max": max(pw) if pw else None}
 
 
-def cpu_reference_step(g, p, m_sub, threads=None):
-    """One bounded run of the reference's CPU search on the first m_sub SNPs."""
+def _oracle_module():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
     import oracle
+    return oracle
+
+
+def cpu_reference_step(g, p, m_sub, threads=None, block=(64, 16)):
+    """One bounded run of the reference's CPU search on the first m_sub SNPs."""
+    import numpy as np
+    oracle = _oracle_module()
     binary = oracle.best_ref_binary()
     if binary is None:
         return None
@@ -114,51 +119,95 @@ def cpu_reference_step(g, p, m_sub, threads=None):
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "geno.bin")
         oracle.write_geno_file(path, sub, p)
-        r = oracle.run_ref_file(binary, path, sub.shape[0], m_sub, 64, 16, threads=threads, timeout=600)
+        r = oracle.run_ref_file(binary, path, sub.shape[0], m_sub, block[0], block[1], threads=threads, timeout=600)
     ts = m_sub * (m_sub - 1) * (m_sub - 2) // 6 * sub.shape[0]
     return {"value": ts / r["wall_search_s"], "wall_s": r["wall_search_s"], "threads": r["threads"],
-            "binary": binary, "ijk": r["ijk"], "triplet_samples": ts}
+            "binary": binary, "ijk": r["ijk"], "triplet_samples": ts, "block": list(block), "m_sub": m_sub}
 
 
-def cpu_sample_snps():
-    """SNP count of one bounded CPU step: ~5-15 s of reference work on this host."""
-    cores = os.cpu_count() or 1
-    rate = 1.2e10 * cores  # triplet*samples/s per core of the reference's AVX-512 search (measured on a 8-core host)
-    for m_sub in (1024, 768, 640, 512):
-        if m_sub * (m_sub - 1) * (m_sub - 2) / 6 * 16384 / rate <= 12.0:
-            return m_sub
-    return 384
+# block_pac x block_snp of the reference's blocked search (CPU/v4_popc_avx512.cpp:4600-4601)
+CPU_BLOCKS = [(32, 16), (32, 32), (64, 16), (64, 32), (128, 16), (128, 32)]
+
+
+def cpu_baseline_protocol(g, p, threads=None):
+    """The reference's CPU search timed by a bounded protocol: sweep the six block shapes on
+    the first 512 SNPs, then time the best shape on the first 512, 768 and 1024 SNPs to check
+    that triplet*samples/s is flat in the subset size (the rate the full search would have).
+    Returns None when no reference binary is built."""
+    sweep = []
+    for blk in CPU_BLOCKS:
+        r = cpu_reference_step(g, p, 512, threads, blk)
+        if r is None:
+            return None
+        sweep.append(r)
+    best = max(sweep, key=lambda r: r["value"])
+    flat = [best] + [cpu_reference_step(g, p, m, threads, tuple(best["block"])) for m in (768, 1024)]
+    rates = [r["value"] for r in flat]
+    return {"best": max(flat, key=lambda r: r["value"]), "block": best["block"],
+            "block_sweep_m512": {f"{r['block'][0]}/{r['block'][1]}": r["value"] for r in sweep},
+            "flatness": {str(r["m_sub"]): r["value"] for r in flat},
+            "flatness_spread": (max(rates) - min(rates)) / max(rates), "threads": best["threads"],
+            "binary": best["binary"], "rate": max(rates),
+            "wall_s": sum(r["wall_s"] for r in sweep + flat[1:])}
+
+
+def reference_matrix(cfg):
+    """The workload's matrix from the oracle's restatement of the seeded generator (no product
+    library is loaded by the reference arm), checked against the recorded digest."""
+    import hashlib
+    import numpy as np
+    oracle = _oracle_module()
+    g, p = oracle.gen_hwe(cfg["seed"], cfg["n_samples"], cfg["n_snps"], cfg["n_cases"], cfg["maf"], cfg["planted"],
+                          cfg["effects"])
+    try:
+        rec = json.load(open(os.path.join(ROOT, "tests", "golden", "ref_best.json")))
+        for v in rec.values():
+            if v["seed"] == cfg["seed"] and v["n_snps"] == cfg["n_snps"] and v["n_samples"] == cfg["n_samples"]:
+                assert hashlib.sha256(np.ascontiguousarray(g).tobytes()).hexdigest() == v["geno_sha256"]
+                break
+    except OSError:
+        pass
+    return g, p
 
 
 def run_reference(args, rank, world):
-    from epik2 import workloads as W
-    import epik2
+    sys.path.insert(0, os.path.join(ROOT, "cross-dpc-episdet_b200", "epik2"))
+    import workloads as W  # the workload table only; the product library is not loaded
     if rank != 0:
         return 0
     cfg = W.PLAIN_LARGE
-    g, p = W.generate(cfg)
-    m_sub = cpu_sample_snps()
-    for _ in range(args.warmup):
-        r = cpu_reference_step(g, p, min(m_sub, 256))
-        if r is None:
-            print(json.dumps({"impl": "reference", "unavailable": "reference CPU harness not built"}))
-            return 0
+    g, p = reference_matrix(cfg)
+    proto = cpu_baseline_protocol(g, p)  # block sweep + flatness check; also warms the host
+    if proto is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU harness not built"}))
+        return 0
+    # each step: the first m_sub SNPs (the rate is flat in the subset size, see "flatness"),
+    # sized to about 3 s of host work so that --steps K ends within minutes
+    m_sub = 512
+    for m in (640, 768, 1024):
+        if m * (m - 1) * (m - 2) / 6 * cfg["n_samples"] / proto["rate"] <= 3.0:
+            m_sub = m
+    for _ in range(max(0, args.warmup - 1)):
+        cpu_reference_step(g, p, 256, block=tuple(proto["block"]))
     walls, ts_total, thr = [], 0, None
     for _ in range(args.steps):
-        r = cpu_reference_step(g, p, m_sub)
+        r = cpu_reference_step(g, p, m_sub, block=tuple(proto["block"]))
         walls.append(r["wall_s"])
         ts_total += r["triplet_samples"]
         thr = r["threads"]
     value = ts_total / sum(walls)
     sample = (f"{cfg['name']}: first {m_sub} SNPs x {cfg['n_samples']} samples per step "
-              f"({r['binary']} search, C({m_sub},3) triplets)")
+              f"({r['binary']} search, C({m_sub},3) triplets, block {proto['block'][0]}/{proto['block'][1]}, "
+              f"the best of the 6-shape sweep)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(walls) / len(walls),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded Hardy-Weinberg, planted triplet)",
             "config": {"workload": cfg["name"], "form": "plain", "sample_snps": m_sub, "step": "bounded CPU sample",
                        "parallelism": "OpenMP host threads"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "reference", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "reference", "sample": sample,
+                             "block_sweep_m512": proto["block_sweep_m512"], "flatness": proto["flatness"],
+                             "flatness_spread": proto["flatness_spread"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -340,12 +389,32 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        m_sub = cpu_sample_snps()
-        r = cpu_reference_step(g, p, m_sub)
-        if r is not None:
-            cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
-                   "sample": f"first {m_sub} SNPs x {S} samples of the same matrix, {r['binary']} "
-                             f"(reference OpenMP search), {r['wall_s']:.2f} s"}
+        proto = cpu_baseline_protocol(g, p)
+        if proto is not None:
+            b = proto["best"]
+            cpu = {"value": proto["rate"], "unit": UNIT, "cores": proto["threads"], "kind": "reference",
+                   "sample": (f"first M' SNPs x {S} samples of the same matrix, {proto['binary']} (reference "
+                              f"OpenMP search): block_pac/block_snp swept over {len(CPU_BLOCKS)} shapes at M'=512, "
+                              f"best {proto['block'][0]}/{proto['block'][1]} timed at M' = 512, 768, 1024; value = "
+                              f"the highest rate ({b['m_sub']} SNPs), {proto['wall_s']:.1f} s of CPU runs"),
+                   "block_sweep_m512": proto["block_sweep_m512"], "flatness": proto["flatness"],
+                   "flatness_spread": proto["flatness_spread"]}
+
+    ctx.close()
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        # the other forms of the north star, bounded (about 1.5 minutes together), after the
+        # timed region: batched, precision and serving
+        forms = {}
+        for name, fn in (("precision", precision_form), ("batched", batched_form), ("serving", serving_form)):
+            t0 = time.perf_counter()
+            try:
+                forms[name] = fn()
+            except Exception as e:  # a form that fails is reported, not fatal to the plain line
+                forms[name] = {"error": f"{type(e).__name__}: {e}"}
+            forms[name]["bench_wall_s"] = time.perf_counter() - t0
+        if "value" in forms.get("batched", {}):
+            forms["batched"]["speedup_vs_plain_large"] = forms["batched"]["value"] / value
 
     if rank == 0:
         line = {
@@ -371,9 +440,9 @@ def run_ours(args, rank, world, local_rank):
             "scan_latency_ms": {"p50": float(np.percentile(kernel_ms, 50)), "p99": float(np.percentile(kernel_ms, 99)),
                                 "what": "device time of one step's search kernel"},
             "best_in_last_step": {"score": bests[-1][0], "ijk": list(bests[-1][1])},
+            "forms": forms,
         }
         print(json.dumps(line))
-    ctx.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
@@ -389,10 +458,11 @@ def _clock_ctx():
     return ClockSampler(pci)
 
 
-def run_batched(args):
+def batched_form(steps=3, warmup=1):
     """Batched workload: 96 datasets (SNPs log-uniform 128..1536, samples log-uniform
-    1000..12000, case fraction 0.3..0.7) in one graph-captured tensor-core launch, against
-    the same datasets scanned one by one (one epik2_scan each)."""
+    1000..12000, case fraction 0.3..0.7) in one graph-captured tensor-core launch sequence,
+    against the same datasets scanned one by one (one epik2_scan each) and against the plain
+    form's rate on plain-large."""
     import numpy as np
     import epik2
     from epik2 import workloads as W
@@ -404,15 +474,17 @@ def run_batched(args):
         g, p = W.generate(sp)
         ids.append(ctx.load(g, p))
         ts_total += epik2.n_triplets(sp["n_snps"]) * sp["n_samples"]
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         ctx.scan_batch(ids)
         for d in ids:
             ctx.scan(d)
     sampler = _clock_ctx()
     sampler.start()
-    batch_ms, obo_ms, obo_wall = [], [], []
-    for _ in range(args.steps):
+    batch_ms, batch_wall, obo_ms, obo_wall = [], [], [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
         best_b = ctx.scan_batch(ids)
+        batch_wall.append((time.perf_counter() - t0) * 1e3)
         batch_ms.append(ctx.stats()["last_scan_kernel_ms"])
         t0 = time.perf_counter()
         k_ms = 0.0
@@ -424,25 +496,22 @@ def run_batched(args):
         obo_ms.append(k_ms)
     clocks = sampler.stop()
     same = all(a.ijk == b.ijk and a.score == b.score for a, b in zip(best_b, best_o))
+    ctx.close()
     v_b = ts_total / (np.median(batch_ms) / 1e3)
     v_o = ts_total / (np.median(obo_wall) / 1e3)
-    line = {"metric": METRIC, "value": v_b, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": float(np.median(batch_ms)), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic (96 seeded Hardy-Weinberg datasets)",
-            "config": {"workload": "batched 96 datasets", "form": "batched",
-                       "triplet_samples_per_step": ts_total, "step": "one batched launch over all 96 datasets"},
+    return {"value": v_b, "unit": UNIT, "ms_per_step": float(np.median(batch_ms)),
+            "wall_ms_per_step": float(np.median(batch_wall)), "steps": steps,
+            "triplet_samples_per_step": ts_total, "datasets": len(specs),
             "one_by_one": {"value": v_o, "ms_per_step": float(np.median(obo_wall)),
                            "kernel_ms_per_step": float(np.median(obo_ms)),
                            "what": "96 separate epik2_scan calls, wall time (host setup, launches, syncs)"},
-            "speedup_vs_one_by_one": v_b / v_o, "results_identical": same, "clocks": clocks}
-    print(json.dumps(line))
-    ctx.close()
-    return 0
+            "speedup_vs_one_by_one": v_b / v_o, "results_identical_to_one_by_one": same, "clocks": clocks}
 
 
-def run_precision(args):
-    """Precision workload (2048 SNPs x 8192 samples, three planted triplets): plain FP32
-    search vs search + per-warp top-32 + FP64 rescore on the GPU."""
+def precision_form(steps=3, warmup=1):
+    """Precision workload (2048 SNPs x 8192 samples, three planted triplets): plain FP32 search
+    vs search + per-warp top-32 + FP64 rescore on the GPU; the FP64 top-32 (set and order) is
+    compared with the FP64 oracle's, recorded in tests/golden/precision_top32.json."""
     import numpy as np
     import epik2
     from epik2 import workloads as W
@@ -451,54 +520,57 @@ def run_precision(args):
     ctx = epik2.Context(0)
     did = ctx.load(g, p)
     ts = epik2.n_triplets(cfg["n_snps"]) * cfg["n_samples"]
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         ctx.scan(did)
         ctx.scan_topk(did, 32, rescore_fp64=1)
     plain_ms, prec_ms = [], []
-    for _ in range(args.steps):
+    for _ in range(steps):
         t0 = time.perf_counter()
         b = ctx.scan(did)
         plain_ms.append((time.perf_counter() - t0) * 1e3)
         t0 = time.perf_counter()
         top = ctx.scan_topk(did, 32, rescore_fp64=1)
         prec_ms.append((time.perf_counter() - t0) * 1e3)
-    err = [abs(t.score - t.score_fp64) / t.score_fp64 for t in top]
-    line = {"metric": METRIC, "value": ts / (np.median(prec_ms) / 1e3), "unit": UNIT, "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median(prec_ms)),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 counts, f32 K2, f64 rescore",
-            "data": "synthetic (seeded Hardy-Weinberg, MAF 0.01..0.5, planted triplets at 0.6/0.7/0.8)",
-            "config": {"workload": cfg["name"], "form": "precision", "top_k": 32},
-            "plain": {"value": ts / (np.median(plain_ms) / 1e3), "ms_per_step": float(np.median(plain_ms))},
-            "k2_rel_error_fp32_vs_fp64": {"max": max(err), "median": float(np.median(err))},
-            "top1": {"ijk": list(top[0].ijk), "score_fp32": top[0].score, "score_fp64": top[0].score_fp64,
-                     "same_as_plain": top[0].ijk == b.ijk},
-            "top32": [list(t.ijk) for t in top]}
-    print(json.dumps(line))
     ctx.close()
-    return 0
+    err = [abs(t.score - t.score_fp64) / t.score_fp64 for t in top]
+    out = {"value": ts / (np.median(prec_ms) / 1e3), "unit": UNIT, "ms_per_step": float(np.median(prec_ms)),
+           "workload": cfg["name"], "top_k": 32,
+           "plain": {"value": ts / (np.median(plain_ms) / 1e3), "ms_per_step": float(np.median(plain_ms))},
+           "k2_rel_error_fp32_vs_fp64": {"max": max(err), "median": float(np.median(err)), "tolerance": 1e-5},
+           "top1": {"ijk": list(top[0].ijk), "score_fp32": top[0].score, "score_fp64": top[0].score_fp64,
+                    "same_as_plain": top[0].ijk == b.ijk}}
+    try:
+        fx = json.load(open(os.path.join(ROOT, "tests", "golden", "precision_top32.json")))
+        ref = [x["ijk"] for x in fx["top"]]
+        got = [list(t.ijk) for t in top]
+        out["vs_fp64_oracle"] = {"top1_equal": got[0] == ref[0], "top32_set_equal": sorted(got) == sorted(ref),
+                                 "top32_order_equal": got == ref,
+                                 "fp64_scores_bit_equal": all(t.score_fp64 == float.fromhex(x["s64"])
+                                                              for t, x in zip(top, fx["top"]))}
+    except (OSError, KeyError, ValueError):
+        out["vs_fp64_oracle"] = None
+    return out
 
 
-def run_serving(args):
-    """Serving workload: resident matrices A (1024 SNPs x 8192 samples) and B (3072 x
-    4096); Poisson arrivals; each request 16..1000 phenotype-permutation replicates of a
-    random resident matrix, 10% a fresh 256..768-SNP x 4096-sample matrix.  Reports the
-    offered and sustained load, completed/refused requests and p50/p99 latency.  A second
-    run offers half the measured capacity with 16-replicate requests on A (latency at a
-    sustainable rate)."""
+def serving_form(seconds=15.0, drain=15.0, check_requests=6):
+    """Serving workload: resident matrices A (1024 SNPs x 8192 samples) and B (3072 x 4096);
+    Poisson arrivals; each request 16..1000 phenotype-permutation replicates of a random
+    resident matrix, 10% a fresh 256..768-SNP x 4096-sample matrix.  Reports the offered and
+    sustained load, completed/refused requests, p50/p99 latency, the FP32-vs-FP64 K2 error of
+    every result, and a check of the first result of a few completed requests against a plain
+    run of the same phenotype.  A second run offers half the measured capacity with
+    16-replicate requests on A (latency at a sustainable rate)."""
     import numpy as np
     import epik2
     from epik2 import workloads as W
     spec = W.SERVING
     rng = np.random.default_rng(spec["seed"])
+    gens = [W.generate(m) for m in spec["resident"]]
+    pools = [np.stack([rng.permutation(p) for _ in range(256)]) for _, p in gens]
 
-    def serve(rate, duration, req_maker, drain, srv_opts):
+    def serve(rate, duration, req_maker, srv_opts):
         srv = epik2.Server(0, **srv_opts)
-        mats = []
-        for m in spec["resident"]:
-            g, p = W.generate(m)
-            mats.append((srv.add_matrix(g, p), p, m))
-        # pool of permuted phenotypes per matrix (replicates draw consecutive pool entries)
-        pools = [np.stack([rng.permutation(p) for _ in range(256)]) for _, p, _ in mats]
+        mids = [srv.add_matrix(g, p) for g, p in gens]
         t_start = time.perf_counter()
         next_t = t_start
         pending, offered, refused, work_offered = [], 0, 0, 0.0
@@ -509,26 +581,26 @@ def run_serving(args):
                 continue
             next_t += rng.exponential(1.0 / rate)
             offered += 1
-            kind, payload, work = req_maker(mats, pools)
+            kind, payload, work, what = req_maker(mids)
             work_offered += work
             try:
                 rid = srv.submit_replicates(*payload) if kind == "rep" else srv.submit_scan(*payload)
-                pending.append((rid, time.perf_counter()))
+                pending.append((rid, what))
             except epik2.Epik2Error:
                 refused += 1
         t_stop = time.perf_counter()
-        lat, done = [], 0
+        lat, done, errs = [], [], []
         deadline = t_stop + drain
         while pending and time.perf_counter() < deadline:
             still = []
-            for rid, t0 in pending:
+            for rid, what in pending:
                 r = srv.poll(rid)
                 if r is None:
-                    still.append((rid, t0))
-                else:
-                    done += 1
-                    if r[0] == epik2.OK:
-                        lat.append(r[2])
+                    still.append((rid, what))
+                elif r[0] == epik2.OK:
+                    lat.append(r[2])
+                    done.append((what, r[1][0]))
+                    errs += [abs(b.score - b.score_fp64) / b.score_fp64 for b in r[1]]
             pending = still
             time.sleep(0.01)
         st = srv.stats()
@@ -540,40 +612,85 @@ def run_serving(args):
                 "sustained_triplet_samples_per_s": st["triplet_samples"] / wall,
                 "latency_s": {"p50": float(np.percentile(lat, 50)) if lat else None,
                               "p99": float(np.percentile(lat, 99)) if lat else None},
-                "scans_done": st["scans_done"], "launches": st["launches"],
-                "busy_fraction": st["busy_seconds"] / wall}
+                "k2_rel_error_fp32_vs_fp64": {"max": max(errs) if errs else None,
+                                              "median": float(np.median(errs)) if errs else None,
+                                              "results": len(errs)},
+                "scans_done": st["scans_done"], "launches": st["launches"], "max_scans_per_launch": st["max_active"],
+                "busy_fraction": st["busy_seconds"] / wall}, done
 
-    def full_request(mats, pools):
+    def full_request(mids):
         if rng.random() < spec["upload_frac"]:
             m = int(rng.integers(spec["upload_snps"][0], spec["upload_snps"][1] + 1))
             g, p = epik2.generate_hwe(int(rng.integers(1 << 30)), 4096, m, 2048)
-            return "scan", (g, p), epik2.n_triplets(m) * 4096
-        a = int(rng.integers(len(mats)))
+            return "scan", (g, p), epik2.n_triplets(m) * 4096, ("fresh", g, p)
+        a = int(rng.integers(len(mids)))
         n = int(rng.integers(spec["replicates"][0], spec["replicates"][1] + 1))
-        mid, p, m = mats[a]
         start = int(rng.integers(256))
         ph = np.take(pools[a], np.arange(start, start + n) % 256, axis=0)
-        return "rep", (mid, ph), n * epik2.n_triplets(m["n_snps"]) * m["n_samples"]
+        m = spec["resident"][a]
+        return "rep", (mids[a], ph), n * epik2.n_triplets(m["n_snps"]) * m["n_samples"], ("rep", a, start)
 
     srv_opts = dict(rescore_fp64=1, max_queued=20000)
-    full = serve(spec["rate_per_s"], args.serve_seconds, full_request, args.serve_drain, srv_opts)
+    full, done_full = serve(spec["rate_per_s"], seconds, full_request, srv_opts)
     cap = full["sustained_triplet_samples_per_s"] / max(full["busy_fraction"], 1e-9)
     light_work = 16 * epik2.n_triplets(spec["resident"][0]["n_snps"]) * spec["resident"][0]["n_samples"]
     light_rate = max(0.05, 0.5 * cap / light_work)
 
-    def light_request(mats, pools):
-        mid, p, m = mats[0]
+    def light_request(mids):
         start = int(rng.integers(256))
         ph = np.take(pools[0], np.arange(start, start + 16) % 256, axis=0)
-        return "rep", (mid, ph), light_work
+        return "rep", (mids[0], ph), light_work, ("rep", 0, start)
 
-    light = serve(light_rate, args.serve_seconds, light_request, args.serve_drain, srv_opts)
+    light, done_light = serve(light_rate, seconds, light_request, srv_opts)
+    # each checked request's first result against a plain run of its phenotype
+    checked, matched = 0, 0
+    with epik2.Context(0) as ctx:
+        dids = [ctx.load(g, p) for g, p in gens]
+        for what, best in (done_full[:check_requests] + done_light[:2]):
+            if what[0] == "rep":
+                ctx.set_pheno(dids[what[1]], pools[what[1]][what[2] % 256])
+                ref = ctx.scan(dids[what[1]])
+            else:
+                ref = ctx.scan_u8(what[1], what[2])
+            checked += 1
+            matched += int(ref.ijk == best.ijk and ref.score == best.score)
+    return {"offered_load_as_configured": full, "half_capacity_16_replicates_on_A": light,
+            "capacity_triplet_samples_per_s": cap,
+            "per_request_plain_match": {"checked": checked, "matched": matched,
+                                        "what": "first result of each checked request vs epik2_scan of that "
+                                                "phenotype (bit-exact FP32 score and triplet)"}}
+
+
+def run_batched(args):
+    r = batched_form(args.steps, args.warmup)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (96 seeded Hardy-Weinberg datasets)",
+            "config": {"workload": "batched 96 datasets", "form": "batched",
+                       "triplet_samples_per_step": r["triplet_samples_per_step"],
+                       "step": "one batched launch over all 96 datasets"}, "batched": r}
+    print(json.dumps(line))
+    return 0
+
+
+def run_precision(args):
+    r = precision_form(args.steps, args.warmup)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 counts, f32 K2, f64 rescore",
+            "data": "synthetic (seeded Hardy-Weinberg, MAF 0.01..0.5, planted triplets at 0.6/0.7/0.8)",
+            "config": {"workload": r["workload"], "form": "precision", "top_k": 32}, "precision": r}
+    print(json.dumps(line))
+    return 0
+
+
+def run_serving(args):
+    r = serving_form(args.serve_seconds, args.serve_drain)
+    light = r["half_capacity_16_replicates_on_A"]
     line = {"metric": "p50/p99 scan latency; triplet*samples/s", "value": light["latency_s"]["p50"], "unit": "s",
             "higher_is_better": False, "n_gpus": 1, "steps": None, "warmup": None, "vs_baseline": None,
             "dtype": "u32 counts, f32 K2, f64 rescore", "data": "synthetic (seeded Hardy-Weinberg)",
-            "config": {"workload": "serving: resident A 1024x8192, B 3072x4096", "form": "serving"},
-            "offered_load_as_configured": full, "half_capacity_16_replicates_on_A": light,
-            "capacity_triplet_samples_per_s": cap}
+            "config": {"workload": "serving: resident A 1024x8192, B 3072x4096", "form": "serving"}, "serving": r}
     print(json.dumps(line))
     return 0
 
@@ -595,6 +712,8 @@ def main():
     ap.add_argument("--stage-words", type=int, default=0, help="plain form: tensor-core stage depth (0 = tuned)")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-drain", type=float, default=30.0)
+    ap.add_argument("--no-forms", action="store_true",
+                    help="plain form: leave out the bounded batched/precision/serving runs after the timed steps")
     args = ap.parse_args()
     rank, world, local_rank = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     if args.impl == "reference":

@@ -36,6 +36,8 @@ struct epik2_ctx {
   int tc_blocks = 0;            // tensor-core engine grid (one CTA per SM)
   int n_slots = 0;              // per-warp slots, enough for either grid
   int* d_err = nullptr;
+  int64_t wait_limit = 0;       // SM clocks of a bounded device-side wait (0 = kernel default)
+  int test_withhold = 0;        // one-shot test hook of the bounded-wait error path
   int64_t* d_pb_off = nullptr;
   uint32_t* d_pb_ij = nullptr;
   int64_t pb_cap = 0;
@@ -453,6 +455,7 @@ int run_pairs_tc(epik2_ctx* ctx, DevDataset& d) {
   p.counter = ctx->d_counter;
   p.slots = ctx->d_slots;
   p.err = ctx->d_err;
+  p.wait_limit = ctx->wait_limit;
   p.pairs_out = d.pairs;
   CK(ctx, launch_pairs_tc(p, tc_pair_blocks(ctx->tc_blocks), ctx->stream), "pair-margin kernel");
   ctx->stats.kernel_launches += 2;
@@ -533,6 +536,9 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   p.dump_tables = dump_tables;
   p.dump_scores = dump_scores;
   p.err = ctx->d_err;
+  p.wait_limit = ctx->wait_limit;
+  p.test_withhold = pair ? 0 : ctx->test_withhold;
+  if (!pair) ctx->test_withhold = 0;
   CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
   CK(ctx, launch_scan_tc(p, grid, kw, fp4, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
   CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
@@ -763,6 +769,8 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
       TcParams p{};
       p.counter = pl->d_counters + g;
       p.err = ctx->d_err;
+      p.wait_limit = ctx->wait_limit;
+  p.wait_limit = ctx->wait_limit;
       p.jobs = pl->d_jobs;
       p.tiles = pl->d_tiles + pl->group_off[g];
       p.n_jobs = n;
@@ -941,6 +949,19 @@ int epik2_set_stage_words(epik2_ctx* ctx, int stage_words) {
   if (stage_words != 0 && stage_words != 4 && stage_words != 8 && stage_words != 16)
     return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4, 8 or 16");
   ctx->stage_words = stage_words;
+  return EPIK2_OK;
+}
+
+int epik2_set_wait_limit(epik2_ctx* ctx, int64_t sm_clocks) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (sm_clocks < 0) return fail(ctx, EPIK2_E_INVALID, "wait limit must be >= 0");
+  ctx->wait_limit = sm_clocks;
+  return EPIK2_OK;
+}
+
+int epik2_test_withhold_arrival(epik2_ctx* ctx) {
+  if (!ctx) return EPIK2_E_INVALID;
+  ctx->test_withhold = 1;
   return EPIK2_OK;
 }
 

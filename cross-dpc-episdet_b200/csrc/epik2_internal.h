@@ -125,6 +125,10 @@ struct TcParams {
   // pair-margin form (pairs_out != null): tiles (0, j0, k block) write the (j, k) pair
   // counts of both classes instead of scoring triplets
   uint4* pairs_out;
+  // SM clocks a bounded mbarrier wait lasts before the kernel gives up (0 = about 2 s)
+  long long wait_limit;
+  // test hook: CTA 0 withholds one arrival so that its first wait expires (single CTAs)
+  int32_t test_withhold;
 };
 
 // Kernel launchers (scan_int.cu / scan_tc.cu / encode.cu); all asynchronous on `stream`.

@@ -8,16 +8,20 @@
 // library holds until the process exits.
 //
 // Rules of use:
-//   * The first call on a device resolves the array's device address with
+//   * Every call resolves the array's device address on the current device with
 //     cudaGetSymbolAddress (the host-side symbol is only a stand-in, never a device
-//     pointer) and caches it per device; make that first call outside any stream
-//     capture.
+//     pointer), so the address stays right after a device reset or a new primary
+//     context.  No call may run under stream capture: each one waits for its stream and
+//     copies through pageable host buffers, which capture forbids; a capturing stream is
+//     refused with EPIK2_E_INVALID before anything is enqueued.
 //   * All calls share the one array and it keeps the last call's contents; everything
 //     that must start at zero is cleared by each call.  Calls whose GPU work overlaps
 //     (two host threads, or two streams) race on the array; the host side serialises
 //     calls from one process with a mutex, but work on different streams still must not
 //     overlap on the device.
 //   * Shapes whose buffers exceed the array are rejected with EPIK2_E_TOO_LARGE.
+//   * A call that fails after it has enqueued work waits for its stream before it
+//     returns, so the array is idle when the next call starts.
 //   * Nothing here calls cudaMalloc, cudaFree or any allocating routine; host staging
 //     uses fixed static buffers.
 #include <algorithm>
@@ -37,7 +41,6 @@ constexpr int64_t kLutChunk = 16384;
 constexpr int64_t kMaxFirst = 4096;
 
 std::mutex g_mu;
-unsigned char* g_scratch[kMaxDevices] = {};
 int g_blocks[kMaxDevices] = {};
 float g_lut_chunk[kLutChunk];
 int64_t g_pgoff[kMaxFirst + 1];
@@ -109,17 +112,21 @@ extern "C" int epik2_scan_u8_noalloc(const uint8_t* geno, const uint8_t* pheno, 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return EPIK2_E_NO_DEVICE;
   cudaStream_t st = (cudaStream_t)cuda_stream;
-  if (!g_scratch[dev]) {  // one-time set-up on this device (must not run under stream capture)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) return EPIK2_E_CUDA;
+  if (cap != cudaStreamCaptureStatusNone) return EPIK2_E_INVALID;  // waits and pageable copies end a capture
+  if (!g_blocks[dev]) {  // grid size of this device, once
     int major = 0, sms = 0;
     if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess || major != 10)
       return EPIK2_E_NO_DEVICE;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return EPIK2_E_NO_DEVICE;
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return EPIK2_E_CUDA;
     g_blocks[dev] = sms * scan_blocks_per_sm();
-    g_scratch[dev] = (unsigned char*)p;
   }
-  unsigned char* base = g_scratch[dev];
+  // the array's address in the current context (looked up on every call: a device reset
+  // or a new primary context moves it)
+  void* sym = nullptr;
+  if (cudaGetSymbolAddress(&sym, g_noalloc_scratch) != cudaSuccess || !sym) return EPIK2_E_CUDA;
+  unsigned char* base = (unsigned char*)sym;
   const int n_warps = g_blocks[dev] * (kScanThreads / 32);
   const NoAllocLayout L = noalloc_layout(n_samples, n_snps, n_warps);
   if (L.total > (size_t)EPIK2_NOALLOC_SCRATCH_BYTES) return EPIK2_E_TOO_LARGE;
@@ -143,9 +150,15 @@ extern "C" int epik2_scan_u8_noalloc(const uint8_t* geno, const uint8_t* pheno, 
   d.lut = (float*)(base + L.lut);
   uint8_t* d_pheno = base + L.pheno;
 
-#define NA_CK(x)                                 \
-  do {                                           \
-    if ((x) != cudaSuccess) return EPIK2_E_CUDA; \
+  // after the first enqueue a failing step waits for the stream (ignoring its status), so
+  // that no copy or kernel of this call still uses the array when the lock is released
+#define NA_CK(x)                    \
+  do {                              \
+    if ((x) != cudaSuccess) {       \
+      cudaStreamSynchronize(st);    \
+      cudaGetLastError();           \
+      return EPIK2_E_CUDA;          \
+    }                               \
   } while (0)
   NA_CK(cudaMemcpyAsync(d.geno, geno, (size_t)(n_samples * n_snps), cudaMemcpyHostToDevice, st));
   NA_CK(cudaMemcpyAsync(d_pheno, pheno, (size_t)n_samples, cudaMemcpyHostToDevice, st));

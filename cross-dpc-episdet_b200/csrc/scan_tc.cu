@@ -52,7 +52,7 @@ constexpr int kEStride = 132;  // words per row of the epilogue staging buffer (
 constexpr int kLutOff = 2 * 128 * kEStride * 4;
 constexpr int kLutCapacity = (kBarOff - kLutOff) / 4;
 static_assert(kRingBytes <= kBarOff && kLutOff % 16 == 0, "shared-memory layout");
-constexpr long long kWaitLimit = 4000000000LL;  // SM clocks (~2 s) before a wait gives up
+constexpr long long kWaitLimit = 4000000000LL;  // default SM clocks (~2 s) before a wait gives up
 // instruction descriptor: D s32, A/B signed 8-bit, both K-major, N = 256, M = 128
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
 // block-scaled instruction descriptor (kind::mxf4): A/B E2M1, scale factors UE8M0, both
@@ -170,7 +170,7 @@ __device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait with cluster-scope acquire (arrivals come from the other CTA of a pair).
-__device__ __forceinline__ bool bar_wait_cluster(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool bar_wait_cluster(uint32_t bar, uint32_t parity, long long limit) {
   const long long t0 = clock64();
   for (;;) {
     uint32_t ok;
@@ -182,15 +182,15 @@ __device__ __forceinline__ bool bar_wait_cluster(uint32_t bar, uint32_t parity) 
         : "r"(bar), "r"(parity)
         : "memory");
     if (ok) return true;
-    if (clock64() - t0 > kWaitLimit) return false;
+    if (clock64() - t0 > limit) return false;
   }
 }
 
 // Bounded wait for the completion of the mbarrier phase with the given parity.
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, long long limit) {
   const long long t0 = clock64();
   while (!bar_try_wait(bar, parity)) {
-    if (clock64() - t0 > kWaitLimit) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }
@@ -303,6 +303,11 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   const uint32_t bar_tile = bar_full0 + 8 * kStages;  // CTA pairs: the odd CTA's "next tile is set"
   volatile int* abort_flag = &s_abort;
   const bool worker = warp < kTcWarps;
+  const long long wl = p.wait_limit > 0 ? p.wait_limit : kWaitLimit;  // clocks a bounded wait lasts
+  // test hook (single CTAs only): warp 0 of CTA 0 leaves out its "stage stored" arrival of
+  // the first stage, so the issuing warp's wait on that stage expires and the kernel takes
+  // its error exit before any MMA was issued
+  const bool hold_first = !kPair && p.test_withhold != 0 && blockIdx.x == 0 && warp == 0;
   const uint32_t crank = kPair ? cluster_rank() : 0u;  // rank in the CTA pair
   const bool issuer_cta = crank == 0;
 
@@ -413,7 +418,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
           st_cluster_s64(map_cta(smem_u32(&s_tile), 1), d);
           bar_arrive_cluster(map_cta(bar_tile, 1));
         }
-      } else if (!bar_wait_cluster(bar_tile, n_fetch & 1u)) {
+      } else if (!bar_wait_cluster(bar_tile, n_fetch & 1u, wl)) {
         s_abort = 1;
         s_tile = -1;
       }
@@ -505,7 +510,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         const int s = (int)(g % kStages);
         const uint32_t use = g / kStages;
         const bool late =
-            use > 0 && !(kPair ? bar_wait_cluster(bar0 + 8 * s, (use & 1u) ^ 1u) : bar_wait(bar0 + 8 * s, (use & 1u) ^ 1u));
+            use > 0 && !(kPair ? bar_wait_cluster(bar0 + 8 * s, (use & 1u) ^ 1u, wl) : bar_wait(bar0 + 8 * s, (use & 1u) ^ 1u, wl));
         if (__any_sync(kFull, late)) *abort_flag = 1;
         if (__shfl_sync(kFull, *abort_flag, 0)) break;  // warp-uniform
         const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
@@ -556,7 +561,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         for (int r = 0; r < kUB; r++) ck[r] = nk[r];
         fence_proxy_async();
         __syncwarp();
-        if (lane == 0) bar_arrive(bar_full0 + 8 * s);
+        if (lane == 0 && !(hold_first && g == 0)) bar_arrive(bar_full0 + 8 * s);
       }
     } else if (kPair && lane == 0 && !issuer_cta) {
       // the odd CTA of a pair forwards "stage stored" to the issuing CTA: one cluster-scope
@@ -564,7 +569,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       for (int cc = 0; cc < nct; ++cc) {
         const uint32_t g = g_chunk + (uint32_t)cc;
         const int s = (int)(g % kStages);
-        if (!bar_wait(bar_full0 + 8 * s, (g / kStages) & 1u)) {
+        if (!bar_wait(bar_full0 + 8 * s, (g / kStages) & 1u, wl)) {
           *abort_flag = 1;
           break;
         }
@@ -576,7 +581,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         const uint32_t g = g_chunk + (uint32_t)cc;
         const int s = (int)(g % kStages);
         const uint32_t use = g / kStages;
-        if (!(kPair ? bar_wait_cluster(bar_full0 + 8 * s, use & 1u) : bar_wait(bar_full0 + 8 * s, use & 1u))) {
+        if (!(kPair ? bar_wait_cluster(bar_full0 + 8 * s, use & 1u, wl) : bar_wait(bar_full0 + 8 * s, use & 1u, wl))) {
           *abort_flag = 1;
           break;
         }
@@ -612,7 +617,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
 
     // ---- epilogue: TMEM -> shared -> complete tables, score, select ----
     {
-      const bool ok = kPair ? bar_wait_cluster(bar_acc, n_tile & 1u) : bar_wait(bar_acc, n_tile & 1u);
+      const bool ok = kPair ? bar_wait_cluster(bar_acc, n_tile & 1u, wl) : bar_wait(bar_acc, n_tile & 1u, wl);
       if (!ok) *abort_flag = 1;
       __syncthreads();
       if (*abort_flag) break;

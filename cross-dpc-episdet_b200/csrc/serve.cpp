@@ -147,6 +147,7 @@ struct epik2_server {
           if (r->n_admitted < r->n_scans) pending.push_back(r);
         }
         stats.scans_active = (int64_t)batch.size();
+        stats.max_active = std::max(stats.max_active, stats.scans_active);
       }
       if (batch.empty()) {  // queued scans wait for device memory held elsewhere
         std::unique_lock<std::mutex> lk(mu);

@@ -80,7 +80,7 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("rejected", ctypes.c_int64),
                 ("cancelled", ctypes.c_int64), ("scans_queued", ctypes.c_int64), ("scans_active", ctypes.c_int64),
                 ("scans_done", ctypes.c_int64), ("launches", ctypes.c_int64), ("triplet_samples", ctypes.c_double),
-                ("busy_seconds", ctypes.c_double)]
+                ("busy_seconds", ctypes.c_double), ("max_active", ctypes.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -145,6 +145,8 @@ def library():
         "epik2_scan_u8_noalloc": ([p, p, i64, i64, p, ctypes.POINTER(Best)], ctypes.c_int),
         "epik2_set_engine": ([p, ctypes.c_int], ctypes.c_int),
         "epik2_set_stage_words": ([p, ctypes.c_int], ctypes.c_int),
+        "epik2_set_wait_limit": ([p, i64], ctypes.c_int),
+        "epik2_test_withhold_arrival": ([p], ctypes.c_int),
         "epik2_plink_dims": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
                              ctypes.c_int),
         "epik2_read_plink": ([ctypes.c_char_p, ctypes.c_uint8, p, p], ctypes.c_int),
@@ -307,6 +309,14 @@ class Context:
     def set_stage_words(self, stage_words):
         """Default tensor-core stage depth (0 = autotuned; int8 4/8, FP4 8/16)."""
         self._check(self._lib.epik2_set_stage_words(self._h, stage_words))
+
+    def set_wait_limit(self, sm_clocks):
+        """SM clocks a bounded device-side wait lasts before the search gives up (0 = ~2 s)."""
+        self._check(self._lib.epik2_set_wait_limit(self._h, int(sm_clocks)))
+
+    def test_withhold_arrival(self):
+        """Test hook: the next single-CTA tensor-core search times out (EPIK2_E_TIMEOUT)."""
+        self._check(self._lib.epik2_test_withhold_arrival(self._h))
 
     def stats(self):
         st = Stats()

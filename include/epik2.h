@@ -113,6 +113,18 @@ int epik2_set_stage_words(epik2_ctx *ctx, int stage_words);
 int epik2_set_stream(epik2_ctx *ctx, void *cuda_stream);
 int epik2_get_stream(const epik2_ctx *ctx, void **cuda_stream);
 
+/* Bounded device-side waits.  Every mbarrier wait of the tensor-core kernels gives up after
+ * this many SM clocks: the kernel sets an error word, stops taking tiles, frees its tensor
+ * memory and ends; the call returns EPIK2_E_TIMEOUT and the context stays usable (the
+ * reference has no device-side wait to bound).  0 = the default, about 2 s. */
+int epik2_set_wait_limit(epik2_ctx *ctx, int64_t sm_clocks);
+/* Test hook of that error path (no reference counterpart): in the next tensor-core search
+ * that runs on single CTAs (int8, or FP4 at 8 words per stage), one producing warp of the
+ * first CTA leaves out its first "stage stored" arrival, so the issuing warp's wait expires
+ * before any matrix product is issued and the search returns EPIK2_E_TIMEOUT.  One-shot:
+ * the search after it runs normally. */
+int epik2_test_withhold_arrival(epik2_ctx *ctx);
+
 /* Counters kept by the context (no reference counterpart: the reference's only
  * instrument is a TSC timer around its launch loop, GPU/v4.cpp:282, 609). */
 typedef struct {
@@ -252,6 +264,7 @@ typedef struct {
   int64_t launches;
   double triplet_samples; /* completed work */
   double busy_seconds;    /* worker time inside batched launches */
+  int64_t max_active;     /* most scans admitted to one launch so far */
 } epik2_server_stats;
 int epik2_server_create(epik2_server **out, int device, const epik2_server_opts *opts);
 void epik2_server_destroy(epik2_server *srv);
@@ -295,8 +308,11 @@ int epik2_k2_lut(int64_t n_max, float *lut);
  * device array of EPIK2_NOALLOC_SCRATCH_BYTES (64 MiB) that each GPU loading this library
  * holds until the process exits.  Runs on the current device, on `cuda_stream` (NULL =
  * the default stream), and returns once the result is on the host.
- *   - The first call on a device looks up the array's device address; make that first
- *     call before any stream capture.
+ *   - Every call looks up the array's device address in the current context, so it stays
+ *     valid across a device reset.  No call may be stream-captured: each one waits for its
+ *     stream and copies through pageable host memory; a stream under capture is refused
+ *     with EPIK2_E_INVALID before anything is enqueued.
+ *   - A call that fails after enqueuing work waits for its stream before it returns.
  *   - All calls share the array, which keeps the last call's contents (each call clears
  *     what must start at zero).  Calls whose GPU work overlaps race on it.
  *   - Shapes whose buffers do not fit (about n_samples*n_snps + 16*n_snps^2 bytes plus

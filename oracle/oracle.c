@@ -425,3 +425,176 @@ int64_t oracle_scan_fp64_u8(const uint8_t *A, const uint8_t *B, int64_t N, int64
   free(z);
   return T;
 }
+
+/* ------------------------------------------------------------------ */
+/* FP64 top-k over all triplets (precision-form oracle at full size)   */
+/* ------------------------------------------------------------------ */
+
+typedef struct { double s; int64_t t; } oracle_cand;
+
+/* (s, t) orders before (s2, t2): lower FP64 score, ties to the lower lexicographic index. */
+static int cand_before(double s, int64_t t, double s2, int64_t t2) { return s < s2 || (s == s2 && t < t2); }
+
+/* Max-heap of the k best candidates (root = the worst kept). */
+static void heap_offer(oracle_cand *h, int *n, int k, double s, int64_t t) {
+  if (*n < k) {
+    int c = (*n)++;
+    h[c].s = s;
+    h[c].t = t;
+    while (c > 0) {
+      int p = (c - 1) / 2;
+      if (!cand_before(h[p].s, h[p].t, h[c].s, h[c].t)) break;
+      oracle_cand x = h[p]; h[p] = h[c]; h[c] = x;
+      c = p;
+    }
+    return;
+  }
+  if (!cand_before(s, t, h[0].s, h[0].t)) return;
+  h[0].s = s;
+  h[0].t = t;
+  int c = 0;
+  for (;;) {
+    int l = 2 * c + 1, r = l + 1, w = c;
+    if (l < *n && cand_before(h[w].s, h[w].t, h[l].s, h[l].t)) w = l;
+    if (r < *n && cand_before(h[w].s, h[w].t, h[r].s, h[r].t)) w = r;
+    if (w == c) break;
+    oracle_cand x = h[w]; h[w] = h[c]; h[c] = x;
+    c = w;
+  }
+}
+
+static int cand_cmp(const void *a, const void *b) {
+  const oracle_cand *x = (const oracle_cand *)a, *y = (const oracle_cand *)b;
+  if (cand_before(x->s, x->t, y->s, y->t)) return -1;
+  if (cand_before(y->s, y->t, x->s, x->t)) return 1;
+  return 0;
+}
+
+/* The k lowest FP64 K2 scores of all C(M,3) triplets (ties to the lowest index), in order:
+ * out_t[r] = lexicographic triplet index, out_s64[r] = FP64 score, out_ft[r*54..] = table.
+ * Counting is the definitional 27-cell AND3 + popcount of oracle_table (GPU/v2.cpp:288-540)
+ * on the same per-class planes, two 32-bit words at a time; the nine (g_i, g_j) planes of a
+ * pair are formed once and reused for every k.  Returns the number written (min(k, T)). */
+int64_t oracle_topk_fp64_u8(const uint8_t *A, const uint8_t *B, int64_t N, int64_t M, int k, int64_t *out_t,
+                            double *out_s64, uint32_t *out_ft, int n_threads) {
+  int64_t n1 = 0;
+  for (int64_t s = 0; s < N; s++) n1 += (B[s] == 1);
+  int64_t n0 = N - n1;
+  int64_t W[2] = {(n0 + 31) / 32, (n1 + 31) / 32};
+  uint32_t *planes[2];
+  planes[0] = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(M * W[0] * 2 + 1));
+  planes[1] = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(M * W[1] * 2 + 1));
+  oracle_encode(A, B, N, M, planes[0], planes[1], &n1);
+  uint32_t mask[2];
+  oracle_masks(n0, n1, &mask[0], &mask[1]);
+  /* 64-bit words per class: {g0, g1, g2} of 64 samples, g2 masked on the last 32-bit word
+   * and zero past the class */
+  int64_t V[2] = {(W[0] + 1) / 2, (W[1] + 1) / 2};
+  uint64_t *g64[2];
+  for (int c = 0; c < 2; c++) {
+    g64[c] = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(M * V[c] * 3 + 1));
+    for (int64_t m = 0; m < M; m++)
+      for (int64_t v = 0; v < V[c]; v++) {
+        uint64_t g[3] = {0, 0, 0};
+        for (int h = 0; h < 2; h++) {
+          int64_t w = 2 * v + h;
+          if (w >= W[c]) continue;
+          uint32_t a0 = planes[c][(m * W[c] + w) * 2], a1 = planes[c][(m * W[c] + w) * 2 + 1];
+          uint32_t mk = (w == W[c] - 1) ? mask[c] : 0xFFFFFFFFu;
+          g[0] |= (uint64_t)a0 << (32 * h);
+          g[1] |= (uint64_t)a1 << (32 * h);
+          g[2] |= (uint64_t)(~(a0 | a1) & mk) << (32 * h);
+        }
+        for (int q = 0; q < 3; q++) g64[c][(m * V[c] + v) * 3 + q] = g[q];
+      }
+  }
+  (void)oracle_lnfact_fp64(0); /* initialise the table before the parallel region */
+  int64_t T = (M >= 3) ? M * (M - 1) * (M - 2) / 6 : 0;
+  if (k < 1) k = 1;
+  int n_thr = 1;
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+  n_thr = omp_get_max_threads();
+#endif
+  oracle_cand *heaps = (oracle_cand *)malloc(sizeof(oracle_cand) * (size_t)k * (size_t)n_thr);
+  int *heap_n = (int *)calloc((size_t)n_thr, sizeof(int));
+  const int64_t VT = V[0] + V[1];
+#ifdef _OPENMP
+#pragma omp parallel
+#endif
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    oracle_cand *h = heaps + (size_t)k * (size_t)tid;
+    uint64_t *pij = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(9 * VT + 1));
+    uint32_t ft[54];
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic)
+#endif
+    for (int64_t i = 0; i < M - 2; i++) {
+      for (int64_t j = i + 1; j < M - 1; j++) {
+        for (int c = 0; c < 2; c++) {
+          const uint64_t *a = g64[c] + i * V[c] * 3, *b = g64[c] + j * V[c] * 3;
+          uint64_t *dst = pij + (c ? 9 * V[0] : 0);
+          for (int64_t v = 0; v < V[c]; v++)
+            for (int x = 0; x < 3; x++)
+              for (int y = 0; y < 3; y++) dst[v * 9 + 3 * x + y] = a[v * 3 + x] & b[v * 3 + y];
+        }
+        for (int64_t kk = j + 1; kk < M; kk++) {
+          for (int c = 0; c < 2; c++) {
+            const uint64_t *t3 = g64[c] + kk * V[c] * 3;
+            const uint64_t *src = pij + (c ? 9 * V[0] : 0);
+            uint32_t cnt[27];
+            for (int q = 0; q < 27; q++) cnt[q] = 0;
+            for (int64_t v = 0; v < V[c]; v++) {
+              const uint64_t k0 = t3[v * 3], k1 = t3[v * 3 + 1], k2 = t3[v * 3 + 2];
+              for (int xy = 0; xy < 9; xy++) {
+                const uint64_t ab = src[v * 9 + xy];
+                cnt[3 * xy + 0] += (uint32_t)__builtin_popcountll(ab & k0);
+                cnt[3 * xy + 1] += (uint32_t)__builtin_popcountll(ab & k1);
+                cnt[3 * xy + 2] += (uint32_t)__builtin_popcountll(ab & k2);
+              }
+            }
+            memcpy(ft + 27 * c, cnt, sizeof(cnt));
+          }
+          heap_offer(h, &heap_n[tid], k, oracle_k2_fp64(ft), oracle_triplet_index(M, i, j, kk));
+        }
+      }
+    }
+    free(pij);
+  }
+  /* merge the per-thread heaps */
+  oracle_cand *all = (oracle_cand *)malloc(sizeof(oracle_cand) * (size_t)k * (size_t)n_thr + 1);
+  int64_t n_all = 0;
+  for (int t = 0; t < n_thr; t++)
+    for (int q = 0; q < heap_n[t]; q++) all[n_all++] = heaps[(size_t)k * (size_t)t + (size_t)q];
+  qsort(all, (size_t)n_all, sizeof(oracle_cand), cand_cmp);
+  int64_t n_out = n_all < k ? n_all : k;
+  if (n_out > T) n_out = T;
+  for (int64_t r = 0; r < n_out; r++) {
+    out_t[r] = all[r].t;
+    out_s64[r] = all[r].s;
+  }
+  /* tables of the kept triplets, by the per-triplet oracle */
+  if (out_ft) {
+    for (int64_t r = 0; r < n_out; r++) {
+      int64_t t = out_t[r], i = 0, j, kk;
+      /* invert the lexicographic index */
+      while (oracle_triplet_index(M, i + 1, i + 2, i + 3) <= t && i + 1 < M - 2) i++;
+      j = i + 1;
+      while (j + 1 < M - 1 && oracle_triplet_index(M, i, j + 1, j + 2) <= t) j++;
+      kk = j + 1 + (t - oracle_triplet_index(M, i, j, j + 1));
+      oracle_table(planes[0], planes[1], n0, n1, i, j, kk, out_ft + 54 * r);
+    }
+  }
+  free(all);
+  free(heap_n);
+  free(heaps);
+  free(g64[0]);
+  free(g64[1]);
+  free(planes[0]);
+  free(planes[1]);
+  return n_out;
+}

@@ -52,6 +52,8 @@ def lib():
         L.oracle_scan_u8.restype = i64
         L.oracle_scan_fp64_u8.argtypes = [p, p, i64, i64, p, ctypes.c_int]
         L.oracle_scan_fp64_u8.restype = i64
+        L.oracle_topk_fp64_u8.argtypes = [p, p, i64, i64, ctypes.c_int, p, p, p, ctypes.c_int]
+        L.oracle_topk_fp64_u8.restype = i64
         _lib = L
     return _lib
 
@@ -156,6 +158,31 @@ def scan_fp64(A, B, n_threads=0):
     out = np.zeros(max(T, 1), dtype=np.float64)
     lib().oracle_scan_fp64_u8(_ptr(A), _ptr(B), S, M, _ptr(out), n_threads)
     return out[:T]
+
+
+def topk_fp64(A, B, k=32, n_threads=0):
+    """The k lowest FP64 K2 scores over all triplets (ties to the lowest index), in order:
+    dict(ijk=[(i,j,k)...], s64=float64 array, tables=uint32 [k][54])."""
+    A = np.ascontiguousarray(A, dtype=np.uint8)
+    B = np.ascontiguousarray(B, dtype=np.uint8)
+    S, M = A.shape
+    t = np.zeros(k, dtype=np.int64)
+    s64 = np.zeros(k, dtype=np.float64)
+    ft = np.zeros((k, 54), dtype=np.uint32)
+    n = lib().oracle_topk_fp64_u8(_ptr(A), _ptr(B), S, M, k, _ptr(t), _ptr(s64), _ptr(ft), n_threads)
+    ijk = [triplet_of(M, int(x)) for x in t[:n]]
+    return {"ijk": ijk, "s64": s64[:n].copy(), "tables": ft[:n].copy(), "t": t[:n].copy()}
+
+
+def triplet_of(M, t):
+    """(i, j, k) of lexicographic triplet index t among C(M,3)."""
+    i = 0
+    while i + 1 < M - 2 and triplet_index(M, i + 1, i + 2, i + 3) <= t:
+        i += 1
+    j = i + 1
+    while j + 1 < M - 1 and triplet_index(M, i, j + 1, j + 2) <= t:
+        j += 1
+    return (i, j, j + 1 + (t - triplet_index(M, i, j, j + 1)))
 
 
 def triplet_list(M):

@@ -17,6 +17,16 @@ Fixtures:
   ref_best.json       best triplet + exact score bits of the reference's CPU search
                       (v4_popc_avx512 through oracle/ref_harness) on the seeded
                       Hardy-Weinberg workloads, with a sha256 of each input matrix
+  tile_taps.json      sha256 of every triplet's 54-count table and of every FP32 score
+                      recorded from the reference's unblocked search (oracle/ref_tap_tables)
+                      on shapes that span many tensor-core tiles (too large to commit as
+                      arrays), checked here against the oracle
+  precision_top32.json  the 32 lowest FP64 K2 scores of the precision workload (2048 SNPs x
+                      8192 samples) from the FP64 oracle (oracle_topk_fp64_u8), with their
+                      tables; the FP64 top-1 is checked against the reference's best
+
+    python tests/golden/make_golden.py --only tiles     # just tile_taps.json
+    python tests/golden/make_golden.py --only top32     # just precision_top32.json (~6 min)
 """
 import hashlib
 import json
@@ -33,6 +43,8 @@ sys.path.insert(0, os.path.join(REPO, "oracle"))
 import oracle as O  # noqa: E402
 
 REF = os.path.join(REPO, "oracle", "_ref")
+# the reference sources the harness binaries are built from
+REF_SRC = os.environ.get("EPIK2_REF_DIR", "/root/reference")
 
 
 def sha(a):
@@ -65,8 +77,67 @@ def tap_case(name, A, B, mode_gen=None):
     print(f"tap_{name}: N={N} M={M} T={T} {best_line}")
 
 
-def main(long_runs):
-    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle")], check=True)
+# shapes whose searches span many 64-pair x 112-SNP (and 32 x 128) tensor-core tiles:
+# (seed, samples, SNPs, cases) of O.gen_hwe
+TILE_SHAPES = [(102, 1000, 257, 333), (103, 300, 300, 170)]
+
+
+def tap_raw(A, B):
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "tap.bin")
+        gp = os.path.join(td, "geno.bin")
+        O.write_geno_file(gp, A, B)
+        r = subprocess.run([os.path.join(REF, "ref_tap_tables"), "file", gp, str(A.shape[0]), str(A.shape[1]), out],
+                           check=True, capture_output=True, text=True)
+        raw = open(out, "rb").read()
+    N, M, T = (int(x) for x in np.frombuffer(raw[:24], dtype=np.int64))
+    off = 24 + N * M + N
+    tables = np.frombuffer(raw[off:off + T * 216], dtype=np.uint32).reshape(T, 54)
+    scores = np.frombuffer(raw[off + T * 216:off + T * 220], dtype=np.float32)
+    best_line = [l for l in r.stdout.splitlines() if l.startswith("Best SNPs")][0]
+    return tables, scores, best_line
+
+
+def make_tile_taps():
+    out = {}
+    for seed, S, M, cases in TILE_SHAPES:
+        A, B = O.gen_hwe(seed, S, M, cases)
+        tables, scores, best_line = tap_raw(A, B)
+        r = O.scan(A, B, with_tables=True)
+        assert np.array_equal(r["tables"], tables) and np.array_equal(r["scores"].view(np.uint32),
+                                                                      scores.view(np.uint32)), (seed, S, M)
+        out[f"hwe_{S}x{M}_{cases}cases"] = {
+            "seed": seed, "n_samples": S, "n_snps": M, "n_cases": cases, "triplets": int(len(scores)),
+            "geno_sha256": sha(A), "pheno_sha256": sha(B), "tables_sha256": sha(tables.astype("<u4")),
+            "scores_sha256": sha(scores.view(np.uint32).astype("<u4")), "ref_best_line": best_line}
+        print("tile tap", seed, S, M, best_line)
+    json.dump(out, open(os.path.join(HERE, "tile_taps.json"), "w"), indent=1)
+
+
+def make_precision_top32():
+    sys.path.insert(0, os.path.join(REPO, "cross-dpc-episdet_b200"))
+    from epik2 import workloads as W
+    cfg = W.PRECISION
+    A, B = O.gen_hwe(cfg["seed"], cfg["n_samples"], cfg["n_snps"], cfg["n_cases"], cfg["maf"], cfg["planted"],
+                     cfg["effects"])
+    r = O.topk_fp64(A, B, 32)
+    rb = json.load(open(os.path.join(HERE, "ref_best.json")))["precision"]
+    assert rb["geno_sha256"] == sha(A) and list(r["ijk"][0]) == rb["ijk"], (r["ijk"][0], rb["ijk"])
+    lut = O.lut(cfg["n_samples"] + 1)
+    top = [{"ijk": list(ijk), "s64": float(s).hex(), "s32_bits": int(np.float32(O.k2(t, lut)).view(np.uint32)),
+            "table": [int(x) for x in t]} for ijk, s, t in zip(r["ijk"], r["s64"], r["tables"])]
+    json.dump({"workload": cfg["name"], "seed": cfg["seed"], "geno_sha256": sha(A), "pheno_sha256": sha(B),
+               "source": "oracle_topk_fp64_u8 (27-cell AND3+popcount tables, K2 in double)", "top": top},
+              open(os.path.join(HERE, "precision_top32.json"), "w"), indent=0)
+    print("precision top32:", [t["ijk"] for t in top[:4]], "...")
+
+
+def main(long_runs, only=None):
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), f"REF_DIR={REF_SRC}"], check=True)
+    if only == "tiles":
+        return make_tile_taps()
+    if only == "top32":
+        return make_precision_top32()
 
     # 1. reference programs on their own srand(100) data
     kat = {}
@@ -145,4 +216,4 @@ def main(long_runs):
 
 
 if __name__ == "__main__":
-    main("--long" in sys.argv)
+    main("--long" in sys.argv, sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None)

@@ -51,3 +51,29 @@ def test_precision_workload_top1_matches_reference():
     for t, tab in zip(top, tables):
         assert t.score_fp64 == O.k2_fp64(tab)
         assert f32_bits(t.score) == f32_bits(O.k2(tab, O.lut(rec["n_samples"] + 1)))
+
+
+def test_precision_workload_top32_matches_fp64_oracle():
+    """The full precision workload (2048 SNPs x 8192 samples, three planted triplets): the GPU's
+    FP64 top-32 -- per-warp FP32 top-32 lists, every candidate rescored in FP64 on the GPU,
+    ranked by FP64 score -- equals the FP64 oracle's top-32 over all 1.43e9 triplets in set and
+    order, with bit-identical FP64 scores, the reference's FP32 scores and the oracle's tables
+    (tests/golden/precision_top32.json, made by tests/golden/make_golden.py --only top32)."""
+    import hashlib
+    import json
+    import os
+    from conftest import GOLDEN
+    from epik2 import workloads as W
+    fx = json.load(open(os.path.join(GOLDEN, "precision_top32.json")))
+    g, p = W.generate(W.PRECISION)
+    assert hashlib.sha256(np.ascontiguousarray(g).tobytes()).hexdigest() == fx["geno_sha256"]
+    with epik2.Context(0) as ctx:
+        did = ctx.load(g, p)
+        top = ctx.scan_topk(did, 32, rescore_fp64=1)
+        tables = ctx.tables(did, [t.ijk for t in top])
+    assert [list(t.ijk) for t in top] == [x["ijk"] for x in fx["top"]]
+    for t, x, tab in zip(top, fx["top"], tables):
+        assert t.score_fp64 == float.fromhex(x["s64"])
+        assert f32_bits(t.score) == x["s32_bits"]
+        assert tab.tolist() == x["table"]
+        assert abs(t.score - t.score_fp64) / t.score_fp64 <= REL_TOL

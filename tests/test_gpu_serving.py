@@ -95,3 +95,69 @@ def test_cancel_refuse_and_unknown():
         assert st in (epik2.OK, epik2.E_CANCELLED)  # may have run before the cancel landed
         stats = srv.stats()
     assert stats["rejected"] == 1
+
+
+def test_permutation_pvalue_through_the_server_matches_oracle():
+    """Permutation test end to end: the observed phenotype and R = 64 permutation replicates
+    of one resident matrix run through the server; every replicate's best triplet and FP32
+    score equal the oracle's scan of that permuted phenotype bit for bit, and the p-value
+    (1 + #{replicate best <= observed}) / (1 + R) equals the one from the oracle's scores."""
+    g, p = O.gen_hwe(95, 600, 36, 300, planted=[(4, 17, 30)], effects=[0.85])
+    R = 64
+    reps = _perms(p, R, 7)
+    with epik2.Server(0, batch_work=2e9) as srv:
+        m = srv.add_matrix(g, p)
+        rid_obs = srv.submit_replicates(m, p[None, :])
+        rid = srv.submit_replicates(m, reps)
+        st_obs, obs, _ = srv.wait(rid_obs)
+        st, res, _ = srv.wait(rid)
+    assert st_obs == epik2.OK and st == epik2.OK and len(res) == R
+    ref_obs = O.scan(g, p)
+    assert obs[0].ijk == ref_obs["ijk"] and f32_bits(obs[0].score) == f32_bits(ref_obs["score"])
+    ref_scores = []
+    for r, a in zip(reps, res):
+        ref = O.scan(g, r)
+        assert a.ijk == ref["ijk"] and f32_bits(a.score) == f32_bits(ref["score"])
+        ref_scores.append(np.float32(ref["score"]))
+    pv = epik2.perm_pvalue(obs[0].score, [a.score for a in res])
+    pv_ref = (1 + sum(1 for s in ref_scores if s <= np.float32(ref_obs["score"]))) / (1 + R)
+    assert pv == pv_ref
+    assert pv == 1.0 / (1 + R)  # the planted triplet beats every permutation
+
+
+def test_admission_by_free_device_memory():
+    """Admission control on the host: with a reserve that leaves room for about three and a
+    half replicate datasets (each replicate holds its own planes, margins and tables, ~22 MB
+    here), no launch takes more than three scans, every scan still completes with the result
+    of a plain run of its phenotype, and a fresh matrix that could never fit is refused with
+    EPIK2_E_NOMEM."""
+    S, M = 20000, 1000
+    g, p = epik2.generate_hwe(96, S, M, S // 2)
+    reps = _perms(p, 10, 11)
+    page = 2 << 20
+    per = -(-epik2.library().epik2_replicate_bytes(S, M) // page) * page
+    with epik2.Context(0) as probe:  # a context like the server's, to measure what is free
+        free, total = probe.mem_info()
+    reserve = free - epik2.dataset_bytes(S, M) - int(3.5 * per)
+    with epik2.Server(0, batch_work=1e16, hbm_reserve_bytes=reserve) as srv:
+        m = srv.add_matrix(g, p)
+        rid = srv.submit_replicates(m, reps)
+        big_m = 64
+        while epik2.dataset_bytes(4000, big_m) <= total - reserve:
+            big_m *= 2
+        gb = np.zeros((4000, big_m), dtype=np.uint8)
+        pb = np.zeros(4000, dtype=np.uint8)
+        pb[:2000] = 1
+        rid_big = srv.submit_scan(gb, pb)
+        st, res, _ = srv.wait(rid)
+        st_big, _, _ = srv.wait(rid_big)
+        stats = srv.stats()
+    assert st == epik2.OK and len(res) == 10
+    assert st_big == epik2.E_NOMEM
+    assert 1 <= stats["max_active"] <= 3 and stats["launches"] >= 4
+    with epik2.Context(0) as ctx:
+        did = ctx.load(g, p)
+        for r, a in zip(reps, res):
+            ctx.set_pheno(did, r)
+            b = ctx.scan(did)
+            assert a.ijk == b.ijk and f32_bits(a.score) == f32_bits(b.score)

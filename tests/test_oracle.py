@@ -1,4 +1,6 @@
 """The C oracle pinned against fixtures recorded from the reference itself (CPU only)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -80,3 +82,36 @@ def test_hwe_generator_case_count_and_planted_signal():
     assert int(B.sum()) == 1234
     carrier = (A[:, 2] >= 1) & (A[:, 9] >= 1) & (A[:, 15] >= 1)
     assert B[carrier].mean() > B[~carrier].mean() + 0.2
+
+
+@pytest.mark.parametrize("seed,S,M,cases", [(61, 1500, 60, 700), (63, 513, 33, 100), (64, 70, 5, 33), (65, 200, 3, 100)])
+def test_fp64_topk_oracle_matches_exhaustive_fp64_scan(seed, S, M, cases):
+    """oracle_topk_fp64_u8 (pair planes hoisted, 64-bit words) ranks exactly like the
+    per-triplet FP64 scan, and its tables equal oracle_table's."""
+    g, p = O.gen_hwe(seed, S, M, cases, maf=(0.01, 0.5))
+    s64 = O.scan_fp64(g, p)
+    order = np.lexsort((np.arange(len(s64)), s64))[:32]
+    r = O.topk_fp64(g, p, 32)
+    trip = O.triplet_list(M)
+    assert r["ijk"] == [trip[x] for x in order]
+    assert np.array_equal(r["s64"], s64[order])
+    full = O.scan(g, p, with_tables=True)
+    assert np.array_equal(r["tables"], full["tables"][order])
+
+
+def test_precision_top32_fixture_is_self_consistent():
+    """Each recorded table scores to its recorded FP64 and FP32 values, the list is sorted by
+    (FP64 score, index), and its first triplet is the reference's best on that workload."""
+    import json
+    from conftest import GOLDEN, ref_best
+    fx = json.load(open(os.path.join(GOLDEN, "precision_top32.json")))
+    assert len(fx["top"]) == 32
+    lut = O.lut(8192 + 1)
+    keys = []
+    for x in fx["top"]:
+        t = np.array(x["table"], dtype=np.uint32)
+        assert O.k2_fp64(t) == float.fromhex(x["s64"])
+        assert int(np.float32(O.k2(t, lut)).view(np.uint32)) == x["s32_bits"]
+        keys.append((float.fromhex(x["s64"]), O.triplet_index(2048, *x["ijk"])))
+    assert keys == sorted(keys)
+    assert fx["top"][0]["ijk"] == ref_best()["precision"]["ijk"]
