@@ -249,6 +249,9 @@ def run_ours(args, rank, world, local_rank):
     if args.stage_words:
         ctx.set_stage_words(args.stage_words)
         tune = dict(tune, stage_words=args.stage_words)
+    if args.pair_tile:
+        ctx.set_pair_tile(args.pair_tile)
+        tune = dict(tune, pair_tile=args.pair_tile)
     engine_tc = tune["engine"] in (epik2.ENGINE_TC, epik2.ENGINE_TC_FP4)
     engine_fp4 = tune["engine"] == epik2.ENGINE_TC_FP4
     flush = torch.empty(args.flush_mb << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
@@ -426,12 +429,15 @@ def run_ours(args, rank, world, local_rank):
                        "n_cases": info["n_cases"], "step": f"1/{parts} of the triplet space (first-index shard)",
                        "l2": f"flushed before every step ({args.flush_mb} MiB write)",
                        "parallelism": f"{world} GPU(s), shard-parallel",
-                       "engine": ("tensor cores (tcgen05 %s), %d words per stage"
-                                  % ("block-scaled FP4" if engine_fp4 else "int8", tune["stage_words"])) if engine_tc
+                       "engine": ("tensor cores (tcgen05 %s), %d words per stage, %d SNPs j per tile"
+                                  % ("block-scaled FP4" if engine_fp4 else "int8", tune["stage_words"],
+                                     tune["pair_tile"])) if engine_tc
                        else "integer (LOP3+POPC)",
                        "autotune_rates": {"int": tune["rate_int"], "tc_int8_4": tune["rate_tc4"],
-                                          "tc_int8_8": tune["rate_tc8"], "tc_fp4_8": tune["rate_fp4_8"],
-                                          "tc_fp4_16": tune["rate_fp4_16"]}},
+                                          "tc_int8_8": tune["rate_tc8"], "tc_fp4_8_j32": tune["rate_fp4_8"],
+                                          "tc_fp4_8_j64": tune["rate_fp4_8_pair"],
+                                          "tc_fp4_16_j32": tune["rate_fp4_16_single"],
+                                          "tc_fp4_16_j64": tune["rate_fp4_16"]}},
             "roofline": roof,
             "clocks": clocks,
             "gpu_launches": launches,
@@ -710,6 +716,7 @@ def main():
     ap.add_argument("--engine", default="auto", choices=["auto", "int", "tc", "fp4"],
                     help="plain form: search engine (default: the autotuner's choice)")
     ap.add_argument("--stage-words", type=int, default=0, help="plain form: tensor-core stage depth (0 = tuned)")
+    ap.add_argument("--pair-tile", type=int, default=0, help="plain form: SNPs j per tensor-core tile (0 = tuned)")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-drain", type=float, default=30.0)
     ap.add_argument("--no-forms", action="store_true",

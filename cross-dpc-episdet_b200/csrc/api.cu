@@ -32,6 +32,7 @@ struct epik2_ctx {
   // search scratch
   int engine = 0;               // default engine: 0 = auto, 1 = integer, 2 = tensor cores int8, 3 = tensor cores FP4
   int stage_words = 0;          // default tensor-core stage depth: 0 = autotuned
+  int pair_tile = 0;            // default tensor-core pair tile: 0 = autotuned, 32 or 64
   int scan_blocks = 0;          // integer engine grid
   int tc_blocks = 0;            // tensor-core engine grid (one CTA per SM)
   int n_slots = 0;              // per-warp slots, enough for either grid
@@ -65,7 +66,7 @@ constexpr size_t kMaxPlans = 32;  // cached batched plans per context
 
 struct BatchPlan {
   int64_t n_tiles = 0;
-  std::vector<int> group_code;           // stage_words * 2 + FP4 of each launch group
+  std::vector<int> group_code;           // tc_code() of each launch group
   std::vector<int64_t> group_off;        // tiles of group g: [group_off[g], group_off[g+1])
   unsigned long long* d_counters = nullptr;  // one tile counter per group
   int32_t n_jobs = 0;
@@ -255,11 +256,58 @@ int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
 
 int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_k, int n_warps);
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
-                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4);
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair);
 
 // FP4 accumulators are FP32: counts are exact below 2^24 per class.
 bool fp4_exact(const DevDataset& d) { return d.n_controls < (1 << 24) && d.n_cases < (1 << 24); }
 int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out);
+
+// The tensor-core configurations the autotuner times: format, words per stage, pair tile.
+struct TcConfig {
+  int engine, kw;
+  bool pair;
+};
+constexpr TcConfig kTcConfigs[6] = {{EPIK2_ENGINE_TC, 4, false},     {EPIK2_ENGINE_TC, 8, false},
+                                    {EPIK2_ENGINE_TC_FP4, 8, false}, {EPIK2_ENGINE_TC_FP4, 8, true},
+                                    {EPIK2_ENGINE_TC_FP4, 16, false}, {EPIK2_ENGINE_TC_FP4, 16, true}};
+
+// Measured rate of a configuration in a tuner record (0 = not measured).
+double tune_rate(const epik2_tune& t, int engine, int kw, bool pair) {
+  if (engine == EPIK2_ENGINE_INT) return t.rate_int;
+  if (engine == EPIK2_ENGINE_TC) return pair ? 0.0 : (kw == 4 ? t.rate_tc4 : t.rate_tc8);
+  if (kw == 8) return pair ? t.rate_fp4_8_pair : t.rate_fp4_8;
+  return pair ? t.rate_fp4_16 : t.rate_fp4_16_single;
+}
+
+// Batched-plan code of a configuration.
+int tc_code(int kw, bool fp4, bool pair) { return kw * 4 + (pair ? 2 : 0) + (fp4 ? 1 : 0); }
+
+// Fill in the unset parts (0) of a requested configuration: the tuner's choice when it
+// matches what was asked, else the fastest measured configuration that does.
+void complete_config(const epik2_tune& t, bool can_fp4, int& engine, int& kw, int& pt) {
+  if (engine == 0 && kw == 0 && pt == 0 && (t.engine != EPIK2_ENGINE_TC_FP4 || can_fp4)) {
+    engine = t.engine;
+    kw = t.stage_words;
+    pt = t.pair_tile;
+    return;
+  }
+  double best = -1.0;
+  TcConfig pick{engine ? engine : t.engine, kw, pt == 64};
+  for (const TcConfig& c : kTcConfigs) {
+    if (engine && c.engine != engine) continue;
+    if (kw && c.kw != kw) continue;
+    if (pt && c.pair != (pt == 64)) continue;
+    if (c.engine == EPIK2_ENGINE_TC_FP4 && !can_fp4) continue;
+    const double r = tune_rate(t, c.engine, c.kw, c.pair);
+    if (r > best) {
+      best = r;
+      pick = c;
+    }
+  }
+  engine = pick.engine;
+  kw = pick.kw;
+  pt = pick.pair ? 64 : 32;
+}
 int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* dump_tables, float* dump_scores,
              BestSlot* best_out);
 
@@ -284,28 +332,27 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   int engine = ctx->engine;
   if (opts && opts->engine != 0) engine = opts->engine;
   int kw = (opts && opts->stage_words) ? opts->stage_words : ctx->stage_words;
+  int pt = (opts && opts->pair_tile) ? opts->pair_tile : ctx->pair_tile;
+  if (pt != 0 && pt != 32 && pt != 64) return fail(ctx, EPIK2_E_INVALID, "pair_tile must be 0, 32 or 64");
   if (engine == EPIK2_ENGINE_TC_FP4 && !fp4_exact(d))
     return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
   if (engine == 0 || ((engine == 2 || engine == 3) && kw == 0)) {
     epik2_tune t{};
     int r = tuned(ctx, d, &t);
     if (r) return r;
-    if (engine == 0) {  // a requested stage depth that only one format takes picks that format
-      engine = t.engine;
-      if (kw == 4 && engine == 3) engine = 2;
-      if (kw == 16 && engine == 2 && fp4_exact(d)) engine = 3;
+    if (engine == 0) {  // a requested stage depth or pair tile that one format alone takes picks it
+      if (kw == 4) engine = EPIK2_ENGINE_TC;
+      else if (kw == 16 || pt == 64) engine = fp4_exact(d) ? EPIK2_ENGINE_TC_FP4 : EPIK2_ENGINE_TC;
     }
-    if (kw == 0) {
-      if (engine == t.engine) kw = t.stage_words;
-      else if (engine == 2) kw = t.rate_tc8 >= t.rate_tc4 ? 8 : 4;
-      else if (engine == 3) kw = t.rate_fp4_16 > t.rate_fp4_8 ? 16 : 8;
-    }
+    complete_config(t, fp4_exact(d), engine, kw, pt);
   }
+  if (pt == 0) pt = (engine == EPIK2_ENGINE_TC_FP4 && kw == 16) ? 64 : 32;  // stage depth given, pair tile not
   if (engine == 2 && kw != 0 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
   if (engine == 3 && kw != 0 && kw != 8 && kw != 16)
     return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 8 or 16 with the FP4 engine");
+  if (engine == 2 && pt == 64) return fail(ctx, EPIK2_E_INVALID, "pair tiles of 64 SNPs run on the FP4 format only");
   if (engine == 2 || engine == 3)
-    return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts, kw, engine == 3);
+    return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts, kw, engine == 3, pt == 64);
 
   const int64_t n_first = std::max<int64_t>(ie - ib, 1);
   std::vector<int64_t> off((size_t)n_first + 1, 0);
@@ -469,11 +516,11 @@ int run_pairs_tc(epik2_ctx* ctx, DevDataset& d) {
 // Tensor-core engine: one CTA per SM, tiles = pair blocks (i, j0..j0+31) x k blocks of
 // 128 (int8 format) or 112 (FP4 format) SNPs.
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
-                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4) {
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair) {
   const int64_t m = d.n_snps;
   const int64_t kk = tc_k_per_tile(fp4);
   const int64_t n_kb = (m + kk - 1) / kk;
-  const bool pair = tc_pair(fp4, kw);
+  pair = pair && fp4;
   const int64_t jstep = pair ? 64 : 32;  // SNPs j per tile (a CTA pair takes 64)
   const int grid = pair ? tc_pair_blocks(ctx->tc_blocks) : ctx->tc_blocks;
   std::vector<uint32_t> ij;
@@ -540,7 +587,7 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   p.test_withhold = pair ? 0 : ctx->test_withhold;
   if (!pair) ctx->test_withhold = 0;
   CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
-  CK(ctx, launch_scan_tc(p, grid, kw, fp4, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
+  CK(ctx, launch_scan_tc(p, grid, kw, fp4, pair, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
   CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
   const int n_warps = grid * tc_warps_per_block();
   CK(ctx, launch_reduce_best(ctx->d_slots, n_warps, ctx->d_best, ctx->stream), "reduce kernel");
@@ -582,14 +629,20 @@ int autotune_now(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
   int64_t ie = 1;
   while (ie < m && (triplets_before(m, ie) * 64 < total || triplets_before(m, ie) < 4ll * ctx->tc_blocks * 4096)) ie++;
   const double ts = (double)triplets_before(m, ie) * (double)d.n_samples;
-  // candidates: integer; int8 tensor cores, 4 or 8 words per stage; FP4 tensor cores, 8 or 16
-  double rate[5] = {0, 0, 0, 0, 0};
-  const int eng[5] = {1, 2, 2, 3, 3}, kws[5] = {0, 4, 8, 8, 16};
-  const int n_cand = fp4_exact(d) ? 5 : 3;
+  // candidates: integer; int8 tensor cores, 4 or 8 words per stage (pair tile 32); FP4 tensor
+  // cores, 8 or 16 words per stage, pair tile 32 (one CTA) or 64 (CTA pairs)
+  constexpr int kCand = 7;
+  double rate[kCand] = {0, 0, 0, 0, 0, 0, 0};
+  const int n_cand = fp4_exact(d) ? kCand : 3;
   for (int c = 0; c < n_cand; c++) {
     epik2_opts o{};
-    o.engine = eng[c];
-    o.stage_words = kws[c];
+    if (c == 0) {
+      o.engine = EPIK2_ENGINE_INT;
+    } else {
+      o.engine = kTcConfigs[c - 1].engine;
+      o.stage_words = kTcConfigs[c - 1].kw;
+      o.pair_tile = kTcConfigs[c - 1].pair ? 64 : 32;
+    }
     o.snp_begin = 0;
     o.snp_end = ie;
     BestSlot b{};
@@ -604,12 +657,21 @@ int autotune_now(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
   t.rate_tc4 = rate[1];
   t.rate_tc8 = rate[2];
   t.rate_fp4_8 = rate[3];
-  t.rate_fp4_16 = rate[4];
+  t.rate_fp4_8_pair = rate[4];
+  t.rate_fp4_16_single = rate[5];
+  t.rate_fp4_16 = rate[6];
   int best = 0;
   for (int c = 1; c < n_cand; c++)
     if (rate[c] > rate[best]) best = c;
-  t.engine = eng[best];
-  t.stage_words = best == 0 ? (rate[2] > rate[1] ? 8 : 4) : kws[best];
+  if (best == 0) {  // the integer engine; the stage depth is the faster int8 one
+    t.engine = EPIK2_ENGINE_INT;
+    t.stage_words = rate[2] > rate[1] ? 8 : 4;
+    t.pair_tile = 32;
+  } else {
+    t.engine = kTcConfigs[best - 1].engine;
+    t.stage_words = kTcConfigs[best - 1].kw;
+    t.pair_tile = kTcConfigs[best - 1].pair ? 64 : 32;
+  }
   *out = t;
   return EPIK2_OK;
 }
@@ -636,9 +698,10 @@ int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
 
 // Batched form: build (or reuse) the plan for these datasets, refresh the job table from
 // the datasets' current class split, replay the captured launch sequence.  codes[b] =
-// stage_words * 2 + (FP4 ? 1 : 0) of dataset b; datasets with the same code form a group,
-// one persistent tensor-core launch per group (inside the one graph), each group with its
-// own tile queue (datasets with the most samples first).
+// tc_code() of dataset b's configuration; datasets with the same code form a group, one
+// persistent tensor-core launch per group (inside the one graph), each group with its own
+// tile queue (datasets with the most samples first).  epik2_scan_batch gives every dataset
+// the same code: one group, one launch.
 int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vector<int32_t>& ids,
               const std::vector<int>& codes, bool rescore, epik2_best* out) {
   (void)ids;
@@ -690,7 +753,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     for (int32_t b = 0; b < n; b++) {
       const bool fp4 = codes[b] & 1;
       const int64_t m = ds[b]->n_snps, kk = tc_k_per_tile(fp4), n_kb = (m + kk - 1) / kk;
-      const int64_t jstep = tc_pair(fp4, codes[b] >> 1) ? 64 : 32;
+      const int64_t jstep = (codes[b] & 2) ? 64 : 32;
       auto li = lists.find({m, kk * 2 + (jstep == 64 ? 1 : 0)});
       if (li == lists.end()) {
         ListInfo L{(int64_t)pb_off_all.size(), (int64_t)pb_ij_all.size(), 0, 0};
@@ -776,8 +839,8 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
       p.n_jobs = n;
       p.job_slots = pl->d_job_slots;
       p.n_tiles = nt;
-      const bool gp = tc_pair(group_code[g] & 1, group_code[g] >> 1);
-      e = launch_scan_tc(p, gp ? tc_pair_blocks(grid) : grid, group_code[g] >> 1, group_code[g] & 1, false,
+      const bool gp = (group_code[g] & 2) != 0;
+      e = launch_scan_tc(p, gp ? tc_pair_blocks(grid) : grid, group_code[g] >> 2, group_code[g] & 1, gp, false,
                          ctx->stream);
     }
     if (e == cudaSuccess) e = launch_reduce_jobs(pl->d_job_slots, n, grid, pl->d_results, ctx->stream);
@@ -962,6 +1025,13 @@ int epik2_set_wait_limit(epik2_ctx* ctx, int64_t sm_clocks) {
 int epik2_test_withhold_arrival(epik2_ctx* ctx) {
   if (!ctx) return EPIK2_E_INVALID;
   ctx->test_withhold = 1;
+  return EPIK2_OK;
+}
+
+int epik2_set_pair_tile(epik2_ctx* ctx, int pair_tile) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (pair_tile != 0 && pair_tile != 32 && pair_tile != 64) return fail(ctx, EPIK2_E_INVALID, "pair_tile must be 0, 32 or 64");
+  ctx->pair_tile = pair_tile;
   return EPIK2_OK;
 }
 
@@ -1243,39 +1313,65 @@ int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, cons
     ds.push_back(d);
   }
   CK(ctx, cudaSetDevice(ctx->device), "set device");
-  // format and stage depth per dataset: the requested ones, else the autotuner's choice
-  // for the dataset's shape (int8 when it chose the integer engine, or when a class is too
-  // large for FP4 accumulators).  Datasets with the same choice share one launch.
+  // One configuration (format, stage depth, pair tile) for every dataset, so that all the
+  // tiles drain from one queue in one persistent launch: the requested one, else, among the
+  // tensor-core configurations every dataset can take that match what was requested, the
+  // one with the least predicted time: sum over datasets of work / the autotuner's rate for
+  // the dataset's shape.
   const int engine_req = opts ? opts->engine : 0;
   const int kw_req = opts ? opts->stage_words : 0;
+  const int pt_req = opts ? opts->pair_tile : 0;
   if (engine_req == EPIK2_ENGINE_INT) return fail(ctx, EPIK2_E_INVALID, "the batched form runs on the tensor cores");
   if (engine_req < 0 || engine_req > EPIK2_ENGINE_TC_FP4) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
-  std::vector<int> codes;  // stage_words * 2 + (FP4 ? 1 : 0) per dataset
-  for (DevDataset* d : ds) {
-    const bool can_fp4 = fp4_exact(*d);
-    if (engine_req == EPIK2_ENGINE_TC_FP4 && !can_fp4)
-      return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
-    int engine = engine_req, kw = kw_req;
-    if (engine == 0 || kw == 0) {
+  if (pt_req != 0 && pt_req != 32 && pt_req != 64) return fail(ctx, EPIK2_E_INVALID, "pair_tile must be 0, 32 or 64");
+  bool all_fp4 = true;
+  for (DevDataset* d : ds) all_fp4 = all_fp4 && fp4_exact(*d);
+  if (engine_req == EPIK2_ENGINE_TC_FP4 && !all_fp4)
+    return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
+  TcConfig pick{0, 0, false};
+  bool have = false;
+  if (engine_req != 0 && kw_req != 0 && (pt_req != 0 || engine_req == EPIK2_ENGINE_TC)) {
+    pick = TcConfig{engine_req, kw_req, pt_req == 64};
+    have = true;
+  } else if (engine_req == EPIK2_ENGINE_TC_FP4 && kw_req != 0 && pt_req == 0) {
+    pick = TcConfig{engine_req, kw_req, kw_req == 16};  // stage depth given, pair tile not
+    have = true;
+  } else {
+    std::vector<epik2_tune> tunes;
+    for (DevDataset* d : ds) {
       epik2_tune t{};
       int r = tuned(ctx, *d, &t);
       if (r) return r;
-      if (engine == 0) {  // a requested stage depth that only one format takes picks that format
-        engine = (t.engine == EPIK2_ENGINE_TC_FP4 && can_fp4) ? EPIK2_ENGINE_TC_FP4 : EPIK2_ENGINE_TC;
-        if (kw == 4) engine = EPIK2_ENGINE_TC;
-        if (kw == 16 && can_fp4) engine = EPIK2_ENGINE_TC_FP4;
+      tunes.push_back(t);
+    }
+    double best_time = 0.0;
+    for (const TcConfig& c : kTcConfigs) {
+      if (engine_req && c.engine != engine_req) continue;
+      if (kw_req && c.kw != kw_req) continue;
+      if (pt_req && c.pair != (pt_req == 64)) continue;
+      if (c.engine == EPIK2_ENGINE_TC_FP4 && !all_fp4) continue;
+      double time = 0.0;
+      bool ok = true;
+      for (size_t b = 0; b < ds.size() && ok; b++) {
+        const double rate = tune_rate(tunes[b], c.engine, c.kw, c.pair);
+        const double m = (double)ds[b]->n_snps;
+        ok = rate > 0.0;
+        time += m * (m - 1) * (m - 2) / 6.0 * (double)ds[b]->n_samples / (ok ? rate : 1.0);
       }
-      if (kw == 0) {
-        if (engine == EPIK2_ENGINE_TC_FP4) kw = t.rate_fp4_16 > t.rate_fp4_8 ? 16 : 8;
-        else kw = t.rate_tc8 >= t.rate_tc4 ? 8 : 4;
+      if (ok && (!have || time < best_time)) {
+        best_time = time;
+        pick = c;
+        have = true;
       }
     }
-    const bool fp4 = engine == EPIK2_ENGINE_TC_FP4;
-    if (!fp4 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
-    if (fp4 && kw != 8 && kw != 16)
-      return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 8 or 16 with the FP4 engine");
-    codes.push_back(kw * 2 + (fp4 ? 1 : 0));
   }
+  if (!have) return fail(ctx, EPIK2_E_INVALID, "no tensor-core configuration matches the request");
+  const bool fp4 = pick.engine == EPIK2_ENGINE_TC_FP4;
+  if (!fp4 && pick.kw != 4 && pick.kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
+  if (fp4 && pick.kw != 8 && pick.kw != 16)
+    return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 8 or 16 with the FP4 engine");
+  if (!fp4 && pick.pair) return fail(ctx, EPIK2_E_INVALID, "pair tiles of 64 SNPs run on the FP4 format only");
+  const std::vector<int> codes(ds.size(), tc_code(pick.kw, fp4, pick.pair && fp4));
   return run_batch(ctx, ds, ids, codes, opts && opts->rescore_fp64, out);
 }
 

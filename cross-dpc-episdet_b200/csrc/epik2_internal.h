@@ -142,11 +142,11 @@ cudaError_t launch_tables(const DevDataset& d, const uint32_t* triplets, int64_t
                           cudaStream_t stream);
 cudaError_t launch_rescore(const DevDataset& d, const BestSlot* cand, int64_t n, Rescored* out, cudaStream_t stream);
 int scan_blocks_per_sm();
-cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool dump,
+// pair: FP4 on CTA pairs (clusters of two CTAs, tiles of 64 SNPs j); else one CTA per tile
+// of 32 SNPs j
+cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool pair, bool dump,
                            cudaStream_t stream);
 int tc_k_per_tile(bool fp4);  // SNPs k per tensor-core tile: 128 (int8) or 112 (FP4)
-// FP4 at 16 words per stage runs as CTA pairs (clusters of two, tiles of 64 pairs j).
-bool tc_pair(bool fp4, int words_per_stage);
 int tc_pair_blocks(int sms);  // resident CTAs of the CTA-pair kernel (even)
 // Tile descriptors of one pair-block list (prefix sums pb_off[0..n_pb], (i, j0) pairs) into
 // out[pb_off[b] ...], tagged with `job`.

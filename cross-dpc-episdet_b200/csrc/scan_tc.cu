@@ -919,6 +919,8 @@ cudaError_t tc_configure() {
     cudaError_t e = set_smem_all<4, false, false>();
     if (e == cudaSuccess) e = set_smem_all<8, false, false>();
     if (e == cudaSuccess) e = set_smem_all<8, true, false>();
+    if (e == cudaSuccess) e = set_smem_all<16, true, false>();
+    if (e == cudaSuccess) e = set_smem_all<8, true, true>();
     if (e == cudaSuccess) e = set_smem_all<16, true, true>();
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k_scan_tc<16, true, true, false, false, false, true>,
@@ -938,7 +940,7 @@ static void launch_variant(const TcParams& p, int blocks, bool batched, bool dum
 }
 
 // CTA-pair kernels: clusters of two CTAs
-template <bool kB, bool kD, bool kT, bool kM = false>
+template <int kW, bool kB, bool kD, bool kT, bool kM = false>
 static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t stream) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)blocks);
@@ -952,12 +954,19 @@ static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t strea
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_scan_tc<16, true, true, kB, kD, kT, kM>, p);
+  return cudaLaunchKernelEx(&cfg, k_scan_tc<kW, true, true, kB, kD, kT, kM>, p);
+}
+
+template <int kW>
+static cudaError_t launch_pair_variant(const TcParams& p, int blocks, bool batched, bool dump, bool topk,
+                                       cudaStream_t stream) {
+  if (batched) return launch_pair<kW, true, false, false>(p, blocks, stream);
+  if (dump) return launch_pair<kW, false, true, false>(p, blocks, stream);
+  if (topk) return launch_pair<kW, false, false, true>(p, blocks, stream);
+  return launch_pair<kW, false, false, false>(p, blocks, stream);
 }
 
 int tc_k_per_tile(bool fp4) { return fp4 ? 112 : 128; }
-
-bool tc_pair(bool fp4, int words_per_stage) { return fp4 && words_per_stage == 16; }
 
 // CTAs of the CTA-pair kernel that can be resident at once (even; at most one per SM).
 int tc_pair_blocks(int sms) {
@@ -987,21 +996,20 @@ int tc_pair_blocks(int sms) {
   return blocks;
 }
 
-cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool dump,
+cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool pair, bool dump,
                            cudaStream_t stream) {
   const cudaError_t ce = tc_configure();
   if (ce != cudaSuccess) return ce;
   const bool topk = p.top_k > 1;
   const bool batched = p.jobs != nullptr;
-  if (tc_pair(fp4, words_per_stage)) {
-    cudaError_t e;
-    if (batched) e = launch_pair<true, false, false>(p, blocks & ~1, stream);
-    else if (dump) e = launch_pair<false, true, false>(p, blocks & ~1, stream);
-    else if (topk) e = launch_pair<false, false, true>(p, blocks & ~1, stream);
-    else e = launch_pair<false, false, false>(p, blocks & ~1, stream);
+  if (fp4 && pair) {
+    const cudaError_t e = words_per_stage == 16
+                              ? launch_pair_variant<16>(p, blocks & ~1, batched, dump, topk, stream)
+                              : launch_pair_variant<8>(p, blocks & ~1, batched, dump, topk, stream);
     if (e != cudaSuccess) return e;
   } else if (fp4) {
-    launch_variant<8, true>(p, blocks, batched, dump, topk, stream);
+    if (words_per_stage == 16) launch_variant<16, true>(p, blocks, batched, dump, topk, stream);
+    else launch_variant<8, true>(p, blocks, batched, dump, topk, stream);
   } else {
     if (words_per_stage == 8) launch_variant<8, false>(p, blocks, batched, dump, topk, stream);
     else launch_variant<4, false>(p, blocks, batched, dump, topk, stream);
@@ -1012,7 +1020,7 @@ cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, b
 cudaError_t launch_pairs_tc(const TcParams& p, int blocks, cudaStream_t stream) {
   const cudaError_t ce = tc_configure();
   if (ce != cudaSuccess) return ce;
-  const cudaError_t e = launch_pair<false, false, false, true>(p, blocks & ~1, stream);
+  const cudaError_t e = launch_pair<16, false, false, false, true>(p, blocks & ~1, stream);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 

@@ -65,7 +65,8 @@ class Stats(ctypes.Structure):
 class Tune(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("rate_int", ctypes.c_double),
                 ("rate_tc4", ctypes.c_double), ("rate_tc8", ctypes.c_double), ("rate_fp4_8", ctypes.c_double),
-                ("rate_fp4_16", ctypes.c_double)]
+                ("rate_fp4_16", ctypes.c_double), ("rate_fp4_8_pair", ctypes.c_double),
+                ("rate_fp4_16_single", ctypes.c_double), ("pair_tile", ctypes.c_int32), ("_pad", ctypes.c_int32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -88,7 +89,7 @@ class ServerStats(ctypes.Structure):
 
 class Opts(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("top_k", ctypes.c_int32), ("rescore_fp64", ctypes.c_int32),
-                ("k_strip", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("pair_tile", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("reserved", ctypes.c_int32),
                 ("snp_begin", ctypes.c_int64), ("snp_end", ctypes.c_int64)]
 
 
@@ -146,6 +147,7 @@ def library():
         "epik2_set_engine": ([p, ctypes.c_int], ctypes.c_int),
         "epik2_set_stage_words": ([p, ctypes.c_int], ctypes.c_int),
         "epik2_set_wait_limit": ([p, i64], ctypes.c_int),
+        "epik2_set_pair_tile": ([p, ctypes.c_int], ctypes.c_int),
         "epik2_test_withhold_arrival": ([p], ctypes.c_int),
         "epik2_plink_dims": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
                              ctypes.c_int),
@@ -264,7 +266,7 @@ def n_triplets(m):
 class Context:
     """One device context: owns a CUDA stream and the resident datasets."""
 
-    def __init__(self, device=0, engine=ENGINE_AUTO, stage_words=0):
+    def __init__(self, device=0, engine=ENGINE_AUTO, stage_words=0, pair_tile=0):
         self._lib = library()
         h = ctypes.c_void_p()
         r = self._lib.epik2_create(ctypes.byref(h), device)
@@ -275,6 +277,8 @@ class Context:
             self.set_engine(engine)
         if stage_words:
             self.set_stage_words(stage_words)
+        if pair_tile:
+            self.set_pair_tile(pair_tile)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -309,6 +313,10 @@ class Context:
     def set_stage_words(self, stage_words):
         """Default tensor-core stage depth (0 = autotuned; int8 4/8, FP4 8/16)."""
         self._check(self._lib.epik2_set_stage_words(self._h, stage_words))
+
+    def set_pair_tile(self, pair_tile):
+        """Default tensor-core pair tile (0 = autotuned; 32, or 64 = FP4 on CTA pairs)."""
+        self._check(self._lib.epik2_set_pair_tile(self._h, pair_tile))
 
     def set_wait_limit(self, sm_clocks):
         """SM clocks a bounded device-side wait lasts before the search gives up (0 = ~2 s)."""

@@ -73,10 +73,12 @@ typedef struct {
                           (int8), 3 = tensor cores (block-scaled FP4) */
   int32_t top_k;       /* 0/1 = best only; >1 = keep the top_k lowest FP32 scores */
   int32_t rescore_fp64;/* 1 = rescore the kept candidates in FP64 on the GPU */
-  int32_t k_strip;     /* tuning: SNPs per k-strip (multiple of 32); 0 = autotuned */
+  int32_t pair_tile;   /* tuning, tensor cores: SNPs j per tile, 32 (one CTA) or 64 (a cluster of two
+                          CTAs sharing one tile, FP4 only); 0 = autotuned (with stage_words given and
+                          pair_tile 0: 64 for FP4 at 16 words, else 32) */
   int32_t stage_words;  /* tuning, tensor cores: 32-sample words per pipeline stage, 4 or 8 (int8),
                            8 or 16 (FP4); 0 = autotuned */
-  int32_t blocks_per_sm;  /* tuning: 0 = occupancy-derived */
+  int32_t reserved;    /* must be 0 */
   int64_t snp_begin;   /* restrict the first index i to [snp_begin, snp_end); 0,0 = all */
   int64_t snp_end;
 } epik2_opts;
@@ -106,6 +108,9 @@ int epik2_set_engine(epik2_ctx *ctx, int engine);
  * 0 = autotuned, else 4 or 8 (int8) / 8 or 16 (FP4; 16 runs as clusters of two CTAs that
  * share one 64-pair tile). */
 int epik2_set_stage_words(epik2_ctx *ctx, int stage_words);
+/* Default tensor-core pair tile of the context (used when epik2_opts.pair_tile is 0): 0 =
+ * autotuned, 32 or 64 (64 = FP4 on clusters of two CTAs). */
+int epik2_set_pair_tile(epik2_ctx *ctx, int pair_tile);
 
 /* Run the context's work on a caller-owned stream (e.g. a PyTorch stream); NULL restores
  * the context's own stream.  The library still synchronises that stream before it
@@ -210,31 +215,41 @@ int epik2_scan_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int
 
 /* --------------------------------------------------------------------------------
  * Batched form (no reference counterpart).  One persistent tensor-core launch over many
- * resident datasets: the triplet tiles of all of them go on one shared queue, each CTA
- * folds its candidates into per-dataset slots, and a per-dataset reduction writes
- * out[0..n).  The launch sequence is captured once per set of datasets into a CUDA
- * graph and replayed (phenotype re-encodings via epik2_set_pheno are picked up).  The
- * stage depth is opts->stage_words or, when 0, the autotuner's choice for the largest
- * dataset.  Each result equals epik2_scan on that dataset alone.  At most 512 datasets per
- * call (EPIK2_E_TOO_LARGE beyond).
+ * resident datasets: the triplet tiles of all of them go on one shared queue (datasets with
+ * the most samples first), each CTA folds its candidates into per-dataset slots, and a
+ * per-dataset reduction writes out[0..n).  The launch sequence is captured once per set of
+ * dataset shapes into a CUDA graph and replayed (phenotype re-encodings via epik2_set_pheno
+ * and new datasets of the same shapes are picked up).  One configuration (format, stage
+ * depth, pair tile) serves the whole call: the requested one, else the one with the least
+ * predicted time, sum over datasets of work / the autotuner's rate for the dataset's shape.
+ * Each result equals epik2_scan on that dataset alone.  At most 512 datasets per call
+ * (EPIK2_E_TOO_LARGE beyond).
  * ------------------------------------------------------------------------------ */
 int epik2_scan_batch(epik2_ctx *ctx, const int32_t *dataset_ids, int32_t n, const epik2_opts *opts,
                      epik2_best *out);
 
-/* Autotuner (no reference counterpart).  Times the integer engine, the int8 tensor-core
- * engine at 4 and 8 words per stage and the FP4 tensor-core engine at 8 and 16 words per
- * stage (when its accumulators are exact for the dataset) on a slice of the dataset
- * (about 1/64 of its triplets, at least a few tiles per SM) and caches the fastest per
- * shape bucket (log2 of samples and SNPs); EPIK2_ENGINE_AUTO scans use the cached choice.
- * Reports the choice and the measured rates (triplet*samples/s; 0 = not a candidate). */
+/* Autotuner (no reference counterpart).  Times seven configurations on a slice of the
+ * dataset (about 1/64 of its triplets, at least a few tiles per SM): the integer engine; the
+ * int8 tensor-core engine at 4 and 8 words (128 and 256 samples) per stage; and, when its
+ * accumulators are exact for the dataset, the FP4 tensor-core engine at 8 and 16 words per
+ * stage, each with a pair tile of 32 SNPs j (one CTA) and of 64 (a cluster of two CTAs).
+ * Caches the fastest per shape bucket (log2 of samples and SNPs); EPIK2_ENGINE_AUTO scans and
+ * the batched form use the cached rates.  Reports the choice and the measured rates
+ * (triplet*samples/s; 0 = not a candidate).  The k-strip (SNPs k per tile: 128 int8, 112
+ * FP4) is fixed by the tensor-memory budget: both classes' accumulators and the scale
+ * factors fill 480 of the 512 columns. */
 typedef struct {
   int32_t engine;        /* EPIK2_ENGINE_INT, EPIK2_ENGINE_TC or EPIK2_ENGINE_TC_FP4 */
   int32_t stage_words;   /* tensor-core stage depth chosen (int8: 4 or 8, FP4: 8 or 16) */
   double rate_int;       /* measured rates on the slice */
-  double rate_tc4;
-  double rate_tc8;
-  double rate_fp4_8;
-  double rate_fp4_16;
+  double rate_tc4;       /* int8, 4 words per stage, 32 j */
+  double rate_tc8;       /* int8, 8 words, 32 j */
+  double rate_fp4_8;     /* FP4, 8 words, 32 j */
+  double rate_fp4_16;    /* FP4, 16 words, 64 j (CTA pairs) */
+  double rate_fp4_8_pair;    /* FP4, 8 words, 64 j (CTA pairs) */
+  double rate_fp4_16_single; /* FP4, 16 words, 32 j */
+  int32_t pair_tile;     /* pair tile chosen: 32 or 64 SNPs j */
+  int32_t _pad;
 } epik2_tune;
 int epik2_autotune(epik2_ctx *ctx, int32_t dataset_id, epik2_tune *out);
 

@@ -59,12 +59,14 @@ def pytest_collection_modifyitems(config, items):
 ENGINES = {1: "int", 2: "tc", 3: "fp4"}
 
 
-@pytest.fixture(scope="session", params=[(1, 0), (2, 0), (3, 8), (3, 16)], ids=["int", "tc", "fp4", "fp4pair"])
+@pytest.fixture(scope="session", params=[(1, 0, 0), (2, 0, 0), (3, 8, 32), (3, 16, 64), (3, 8, 64), (3, 16, 32)],
+                ids=["int", "tc", "fp4", "fp4pair", "fp4pair8", "fp4w16"])
 def ctx(request):
-    """A device context per search engine (integer pipe, int8 tensor cores, FP4 tensor
-    cores, FP4 tensor cores on CTA pairs): every test that takes `ctx` runs on all four."""
+    """A device context per search engine: integer pipe; int8 tensor cores; FP4 tensor cores
+    on single CTAs (32 SNPs j per tile) at 8 and 16 words per stage; FP4 on CTA pairs (64 SNPs
+    j per tile) at 16 and 8 words per stage.  Every test that takes `ctx` runs on all six."""
     import epik2
-    c = epik2.Context(0, engine=request.param[0], stage_words=request.param[1])
+    c = epik2.Context(0, engine=request.param[0], stage_words=request.param[1], pair_tile=request.param[2])
     yield c
     c.close()
 
