@@ -367,10 +367,18 @@ def run_ours(args, rank, world, local_rank):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(ext)
         e_trip = 0
+        parts_ms = {"load_wall": 0.0, "upload_device": 0.0, "encode_margins_device": 0.0, "scan_wall": 0.0,
+                    "search_kernel_device": 0.0}
         for t in range(args.warmup, args.warmup + args.steps):
             lo, hi = shard_of(t)
             b = ctx.scan_u8(gn, pn, snp_begin=lo, snp_end=hi)
-            e_trip += ctx.stats()["last_scan_triplets"]
+            st1 = ctx.stats()
+            e_trip += st1["last_scan_triplets"]
+            parts_ms["load_wall"] += st1["last_load_ms"]
+            parts_ms["upload_device"] += st1["last_upload_ms"]
+            parts_ms["encode_margins_device"] += st1["last_prepare_ms"]
+            parts_ms["scan_wall"] += st1["last_scan_wall_ms"]
+            parts_ms["search_kernel_device"] += st1["last_scan_kernel_ms"]
             exchange(b)
         e1.record(ext)
         torch.cuda.synchronize()
@@ -386,9 +394,14 @@ def run_ours(args, rank, world, local_rank):
             e_ms, e_ts = float(a[0]), float(c[1])
         else:
             e_ts = e_trip * S
+        breakdown = {k: v / args.steps for k, v in parts_ms.items()}
+        breakdown["step"] = e_ms / args.steps
+        breakdown["other"] = breakdown["step"] - breakdown["load_wall"] - breakdown["scan_wall"]
         e2e = {"value": e_ts / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": st["h2d_bytes"] // args.steps,
                "d2h_bytes_per_step": st["d2h_bytes"] // args.steps, "gpu_launches": st["kernel_launches"],
-               "entry_point": "epik2_scan_u8"}
+               "entry_point": "epik2_scan_u8", "breakdown_ms_per_step": breakdown,
+               "what": "load_wall = upload + encode + pair margins (host wall); scan_wall = tile list, search, "
+                       "reduction, read-back (host wall); other = the rest of the call (unload) and the loop"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -1,6 +1,7 @@
 // C ABI (include/epik2.h): contexts, resident datasets, the plain search and the
 // parity/inspection entry points.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,11 @@ struct epik2_ctx {
   cudaStream_t stream = nullptr;      // current stream (own or caller's)
   cudaStream_t own_stream = nullptr;
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  cudaEvent_t ev_load[3] = {nullptr, nullptr, nullptr};  // load: before upload, after upload, prepared
+  // host ln n! tables of the last sample count loaded (a matrix of the same shape reuses them)
+  int64_t lut_samples = -1;
+  std::vector<float> lut_host;
+  std::vector<double> lut64_host;
   epik2_stats stats{};
   cudaDeviceProp prop{};
   std::string last_error;
@@ -464,13 +470,12 @@ int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_
 // on; every (j, k), j < k < m_pad, is written once.  Waits for the result (stream sync).
 int run_pairs_tc(epik2_ctx* ctx, DevDataset& d) {
   const int64_t m_pad = d.m_pad, kk = tc_k_per_tile(true);
-  const int64_t n_kb = (m_pad + kk - 1) / kk;
   std::vector<uint32_t> ij;
   std::vector<int64_t> off(1, 0);
   for (int64_t j0 = 0; j0 <= m_pad - 2; j0 += 64) {
     ij.push_back(0);
     ij.push_back((uint32_t)j0);
-    off.push_back(off.back() + (n_kb - (j0 + 1) / kk));
+    off.push_back(off.back() + tiles_of_pair_block(j0, m_pad, kk));
   }
   const int64_t n_pb = (int64_t)off.size() - 1;
   int r = ensure_pb(ctx, std::max<int64_t>(n_pb, 1));
@@ -519,7 +524,6 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
                 float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair) {
   const int64_t m = d.n_snps;
   const int64_t kk = tc_k_per_tile(fp4);
-  const int64_t n_kb = (m + kk - 1) / kk;
   pair = pair && fp4;
   const int64_t jstep = pair ? 64 : 32;  // SNPs j per tile (a CTA pair takes 64)
   const int grid = pair ? tc_pair_blocks(ctx->tc_blocks) : ctx->tc_blocks;
@@ -529,7 +533,7 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
     for (int64_t j0 = i + 1; j0 <= m - 2; j0 += jstep) {
       ij.push_back((uint32_t)i);
       ij.push_back((uint32_t)j0);
-      off.push_back(off.back() + (n_kb - (j0 + 1) / kk));
+      off.push_back(off.back() + tiles_of_pair_block(j0, m, kk));
     }
   const int64_t n_pb = (int64_t)off.size() - 1;
   if (n_pb > ctx->pb_cap || off.back() > ctx->tiles_cap) {
@@ -539,7 +543,7 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
     for (int64_t i = 0; i < m; i++)
       for (int64_t j0 = i + 1; j0 <= m - 2; j0 += jstep) {
         all_pb++;
-        all_tiles += n_kb - (j0 + 1) / kk;
+        all_tiles += tiles_of_pair_block(j0, m, kk);
       }
     int r0 = ensure_pb(ctx, std::max<int64_t>(all_pb, 1));
     if (r0) return r0;
@@ -752,7 +756,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     std::map<std::pair<int64_t, int64_t>, ListInfo> lists;
     for (int32_t b = 0; b < n; b++) {
       const bool fp4 = codes[b] & 1;
-      const int64_t m = ds[b]->n_snps, kk = tc_k_per_tile(fp4), n_kb = (m + kk - 1) / kk;
+      const int64_t m = ds[b]->n_snps, kk = tc_k_per_tile(fp4);
       const int64_t jstep = (codes[b] & 2) ? 64 : 32;
       auto li = lists.find({m, kk * 2 + (jstep == 64 ? 1 : 0)});
       if (li == lists.end()) {
@@ -762,7 +766,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
           for (int64_t j0 = i + 1; j0 <= m - 2; j0 += jstep) {
             pb_ij_all.push_back((uint32_t)i);
             pb_ij_all.push_back((uint32_t)j0);
-            L.tiles += n_kb - (j0 + 1) / kk;
+            L.tiles += tiles_of_pair_block(j0, m, kk);
             pb_off_all.push_back(L.tiles);
             L.n_pb++;
           }
@@ -936,7 +940,9 @@ int epik2_create(epik2_ctx** out, int device) {
   if (ctx->prop.major != 10) return EPIK2_E_NO_DEVICE;  // built for sm_100a only
   if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) return EPIK2_E_CUDA;
   ctx->stream = ctx->own_stream;
-  if (cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev_stop) != cudaSuccess) {
+  if (cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev_stop) != cudaSuccess ||
+      cudaEventCreate(&ctx->ev_load[0]) != cudaSuccess || cudaEventCreate(&ctx->ev_load[1]) != cudaSuccess ||
+      cudaEventCreate(&ctx->ev_load[2]) != cudaSuccess) {
     epik2_destroy(ctx.release());
     return EPIK2_E_CUDA;
   }
@@ -976,6 +982,8 @@ void epik2_destroy(epik2_ctx* ctx) {
   cudaFreeHost(ctx->h_best);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  for (cudaEvent_t e : ctx->ev_load)
+    if (e) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -1107,16 +1115,24 @@ int epik2_load_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int
   d->pairs = (uint4*)(b + L.pairs);
   d->lut = (float*)(b + L.lut);
   d->lut64 = (double*)(b + L.lut64);
-  std::vector<float> lut((size_t)n_samples + 2);
-  build_k2_lut(n_samples + 1, lut.data());
-  std::vector<double> lut64((size_t)n_samples + 2);
-  build_k2_lut64(n_samples + 1, lut64.data());
+  const auto t_load = std::chrono::steady_clock::now();
+  if (ctx->lut_samples != n_samples) {
+    ctx->lut_host.assign((size_t)n_samples + 2, 0.0f);
+    build_k2_lut(n_samples + 1, ctx->lut_host.data());
+    ctx->lut64_host.assign((size_t)n_samples + 2, 0.0);
+    build_k2_lut64(n_samples + 1, ctx->lut64_host.data());
+    ctx->lut_samples = n_samples;
+  }
+  const std::vector<float>& lut = ctx->lut_host;
+  const std::vector<double>& lut64 = ctx->lut64_host;
+  cudaEventRecord(ctx->ev_load[0], ctx->stream);
   cudaError_t e = cudaMemcpyAsync(d->geno, geno, (size_t)(n_samples * n_snps), cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d->lut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d->lut64, lut64.data(), lut64.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
   ctx->stats.h2d_bytes += (uint64_t)(n_samples * n_snps) + lut.size() * 4 + lut64.size() * 8;
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_load[1], ctx->stream);
   if (e != cudaSuccess) {
     cudaFree(d->block);
     return cuda_fail(ctx, e, "upload dataset");
@@ -1126,6 +1142,16 @@ int epik2_load_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int
     cudaFree(d->block);
     return r;
   }
+  // load breakdown: host -> device copies, then encode + margins (encode_with waited for them)
+  float up_ms = 0.0f, prep_ms = 0.0f;
+  if (cudaEventRecord(ctx->ev_load[2], ctx->stream) == cudaSuccess && cudaEventSynchronize(ctx->ev_load[2]) == cudaSuccess) {
+    cudaEventElapsedTime(&up_ms, ctx->ev_load[0], ctx->ev_load[1]);
+    cudaEventElapsedTime(&prep_ms, ctx->ev_load[1], ctx->ev_load[2]);
+  }
+  ctx->stats.last_upload_ms = up_ms;
+  ctx->stats.last_prepare_ms = prep_ms;
+  ctx->stats.last_load_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_load).count();
   const int32_t id = ctx->next_id++;
   ctx->datasets[id] = std::move(d);
   *dataset_id = id;
@@ -1247,7 +1273,10 @@ int epik2_scan(epik2_ctx* ctx, int32_t dataset_id, const epik2_opts* opts, epik2
   epik2_opts o{};
   if (opts) o = *opts;
   if (o.rescore_fp64 && o.top_k < 2) o.top_k = 32;
+  const auto t_scan = std::chrono::steady_clock::now();
   int r = run_scan(ctx, *d, &o, nullptr, nullptr, &b);
+  ctx->stats.last_scan_wall_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_scan).count();
   if (r) return r;
   if (b.key == ~0ull) return fail(ctx, EPIK2_E_INVALID, "no triplet in the requested range");
   if (o.rescore_fp64) {

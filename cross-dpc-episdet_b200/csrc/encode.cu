@@ -40,6 +40,48 @@ __global__ void k_encode(const uint8_t* __restrict__ geno, const int32_t* __rest
   }
 }
 
+// The same encoding, 16 SNPs per thread, for matrices whose rows are whole 16-byte pieces
+// (n_snps a multiple of 16): one 128-bit load per sample gives the thread all 16 genotypes,
+// so a warp reads 512 consecutive bytes of a sample row per load.  Per 32-bit piece,
+// __vcmpeq4 marks the bytes equal to 0 and to 1; bit b of a plane word is sample b of the
+// class word, as in k_encode.  Groups past n_snps (up to m_pad) write zero planes.
+__global__ void k_encode16(const uint8_t* __restrict__ geno, const int32_t* __restrict__ perm,
+                           uint2* __restrict__ planes, int64_t n_snps, int64_t m_pad, int64_t w0, int64_t w1,
+                           int64_t n0, int64_t n1) {
+  const int64_t m0 = 16 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+  if (m0 >= m_pad) return;
+  const int64_t wt = w0 + w1;
+  for (int64_t w = blockIdx.y; w < wt; w += gridDim.y) {
+    const bool cases = w >= w0;
+    const int64_t base = 32 * (cases ? w - w0 : w);
+    const int64_t n_class = cases ? n1 : n0;
+    const int32_t* pc = perm + (cases ? n0 : 0);
+    uint32_t g0[16], g1[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) g0[q] = g1[q] = 0;
+    if (m0 < n_snps) {
+      const int64_t lim = n_class - base < 32 ? n_class - base : 32;
+      for (int64_t b = 0; b < lim; b++) {
+        const int64_t s = pc[base + b];
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(geno + s * n_snps + m0));
+        const uint32_t x[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+          const uint32_t z = __vcmpeq4(x[h], 0u), o = __vcmpeq4(x[h], 0x01010101u);
+#pragma unroll
+          for (int t = 0; t < 4; t++) {
+            g0[4 * h + t] |= ((z >> (8 * t)) & 1u) << b;
+            g1[4 * h + t] |= ((o >> (8 * t)) & 1u) << b;
+          }
+        }
+      }
+    }
+    uint4* dst = reinterpret_cast<uint4*>(planes + w * m_pad + m0);
+#pragma unroll
+    for (int q = 0; q < 8; q++) dst[q] = make_uint4(g0[2 * q], g1[2 * q], g0[2 * q + 1], g1[2 * q + 1]);
+  }
+}
+
 // singles[c][m][g] = popcount over class c's words of plane g of SNP m.
 __global__ void k_singles(const uint2* __restrict__ planes, uint32_t* __restrict__ singles, int64_t m_pad, int64_t w0,
                           int64_t w1) {
@@ -90,10 +132,17 @@ __global__ void k_pairs(const uint2* __restrict__ planes, uint4* __restrict__ pa
 cudaError_t launch_encode(const DevDataset& d, cudaStream_t stream) {
   const int64_t wt = d.w0 + d.w1;
   if (wt == 0 || d.m_pad == 0) return cudaSuccess;
-  dim3 block(256);
-  dim3 grid((unsigned)((d.m_pad + 255) / 256), (unsigned)(wt < 65535 ? wt : 65535));
-  k_encode<<<grid, block, 0, stream>>>(d.geno, d.perm, d.planes, d.n_snps, d.m_pad, d.w0, d.w1, d.n_controls,
+  const bool vec = d.n_snps % 16 == 0 && ((uintptr_t)d.geno % 16) == 0 && ((uintptr_t)d.planes % 16) == 0;
+  if (vec) {  // 16 SNPs per thread
+    const int64_t groups = d.m_pad / 16;
+    dim3 grid((unsigned)((groups + 127) / 128), (unsigned)(wt < 65535 ? wt : 65535));
+    k_encode16<<<grid, 128, 0, stream>>>(d.geno, d.perm, d.planes, d.n_snps, d.m_pad, d.w0, d.w1, d.n_controls,
+                                         d.n_cases);
+  } else {
+    dim3 grid((unsigned)((d.m_pad + 255) / 256), (unsigned)(wt < 65535 ? wt : 65535));
+    k_encode<<<grid, 256, 0, stream>>>(d.geno, d.perm, d.planes, d.n_snps, d.m_pad, d.w0, d.w1, d.n_controls,
                                       d.n_cases);
+  }
   return cudaGetLastError();
 }
 

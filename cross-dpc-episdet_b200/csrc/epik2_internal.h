@@ -89,7 +89,9 @@ struct TcJob {
 };
 
 // Tensor-core tile descriptor: first index i (bits 0-19), first SNP j0 of the pair block
-// (bits 20-39), k block (bits 40-53: k in [kK*kb, kK*kb + kK)), batched job (bits 54-62).
+// (bits 20-39), k block t of the pair block (bits 40-53: k in [k0, k0 + kK) with
+// k0 = j0 + 1 + kK*t, so the blocks of a pair block start at its first valid k), batched job
+// (bits 54-62).
 __host__ __device__ inline uint64_t pack_tile(uint32_t i, uint32_t j0, uint32_t kb, uint32_t job) {
   return (uint64_t)i | ((uint64_t)j0 << 20) | ((uint64_t)kb << 40) | ((uint64_t)job << 54);
 }
@@ -98,10 +100,17 @@ __host__ __device__ inline int tile_j0(uint64_t d) { return (int)((d >> 20) & 0x
 __host__ __device__ inline int tile_kb(uint64_t d) { return (int)((d >> 40) & 0x3FFF); }
 __host__ __device__ inline int tile_job(uint64_t d) { return (int)((d >> 54) & 0x1FF); }
 constexpr int kMaxBatchJobs = 512;  // datasets per batched launch (9 descriptor bits)
+// First SNP k of tile descriptor d (kK SNPs k per tile).
+__host__ __device__ inline int tile_k0(uint64_t d, int kK) { return tile_j0(d) + 1 + kK * tile_kb(d); }
+// Tiles of the pair block starting at SNP j0 whose k run over [j0 + 1, k_end).
+__host__ __device__ inline int64_t tiles_of_pair_block(int64_t j0, int64_t k_end, int64_t kK) {
+  return k_end > j0 + 1 ? (k_end - j0 - 1 + kK - 1) / kK : 0;
+}
 
-// Tensor-core engine parameters (scan_tc.cu).  Tiles: for each pair block (i, j0..j0+31)
-// the k blocks [kK*kb, kK*kb+kK) with kb from (j0+1)/kK to ceil(m/kK)-1 (kK = 128 int8,
-// 112 FP4), one descriptor (pack_tile) per tile, taken in order from a shared counter.
+// Tensor-core engine parameters (scan_tc.cu).  Tiles: for each pair block (i, j0..j0+31,
+// or j0..j0+63 on CTA pairs) the k blocks [j0+1+kK*t, j0+1+kK*(t+1)) covering k < m (kK =
+// 128 int8, 112 FP4), one descriptor (pack_tile) per tile, taken in order from a shared
+// counter.
 struct TcParams {
   const uint2* planes;
   const uint32_t* singles;

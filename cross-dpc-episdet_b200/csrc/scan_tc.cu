@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     }
     if (desc < 0) break;
     // this CTA's pairs: j0 .. j0+31 (pairs of a CTA pair: 32*rank further)
-    const int i = tile_i(desc), j0 = tile_j0(desc) + 32 * (int)crank, k0 = kK * tile_kb(desc);
+    const int i = tile_i(desc), j0 = tile_j0(desc) + 32 * (int)crank, k0 = tile_k0(desc, kK);
     const int job = kBatched ? tile_job(desc) : 0;
     JobView jv;
     if (kBatched) {
@@ -821,16 +821,16 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
 }
 
 // Tile descriptors of one pair-block list: pair block b = (i, j0) holds the tiles
-// [pb_off[b], pb_off[b+1]) with k blocks (j0+1)/kK, (j0+1)/kK + 1, ...; one thread per
-// pair block writes them to out[pb_off[b] ...].
+// [pb_off[b], pb_off[b+1]) with k blocks t = 0, 1, ... (k from j0 + 1 + kK*t); one thread
+// per pair block writes them to out[pb_off[b] ...].
 __global__ void k_expand_tiles(const int64_t* __restrict__ pb_off, const uint32_t* __restrict__ pb_ij, int64_t n_pb,
                                int kK, int job, uint64_t* __restrict__ out) {
+  (void)kK;
   const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n_pb) return;
   const uint32_t i = pb_ij[2 * b], j0 = pb_ij[2 * b + 1];
-  const uint32_t kb0 = (j0 + 1) / (uint32_t)kK;
   const int64_t t0 = pb_off[b], n = pb_off[b + 1] - t0;
-  for (int64_t t = 0; t < n; t++) out[t0 + t] = pack_tile(i, j0, kb0 + (uint32_t)t, (uint32_t)job);
+  for (int64_t t = 0; t < n; t++) out[t0 + t] = pack_tile(i, j0, (uint32_t)t, (uint32_t)job);
 }
 
 cudaError_t launch_expand_tiles(const int64_t* pb_off, const uint32_t* pb_ij, int64_t n_pb, bool fp4, int job,

@@ -56,7 +56,9 @@ class Best(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("kernel_launches", ctypes.c_uint64), ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
                 ("last_scan_kernel_ms", ctypes.c_double), ("last_scan_triplets", ctypes.c_int64),
-                ("last_scan_words", ctypes.c_int64)]
+                ("last_scan_words", ctypes.c_int64), ("last_load_ms", ctypes.c_double),
+                ("last_upload_ms", ctypes.c_double), ("last_prepare_ms", ctypes.c_double),
+                ("last_scan_wall_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -139,6 +139,10 @@ typedef struct {
   double last_scan_kernel_ms;   /* device time of the last search kernel (CUDA events on its stream) */
   int64_t last_scan_triplets;   /* triplets scored by the last search */
   int64_t last_scan_words;      /* 32-sample class words per triplet in the last search (both classes) */
+  double last_load_ms;          /* host wall time of the last epik2_load_u8 (upload, encode, margins) */
+  double last_upload_ms;        /* device time of its host -> device copies (CUDA events) */
+  double last_prepare_ms;       /* device time of its encode and margin kernels, to their completion */
+  double last_scan_wall_ms;     /* host wall time of the last epik2_scan (setup, search, reduction, read-back) */
 } epik2_stats;
 int epik2_get_stats(const epik2_ctx *ctx, epik2_stats *out);
 int epik2_reset_stats(epik2_ctx *ctx);
