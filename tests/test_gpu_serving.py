@@ -102,7 +102,9 @@ def test_permutation_pvalue_through_the_server_matches_oracle():
     of one resident matrix run through the server; every replicate's best triplet and FP32
     score equal the oracle's scan of that permuted phenotype bit for bit, and the p-value
     (1 + #{replicate best <= observed}) / (1 + R) equals the one from the oracle's scores."""
-    g, p = O.gen_hwe(95, 600, 36, 300, planted=[(4, 17, 30)], effects=[0.85])
+    # common alleles (MAF 0.3..0.5) make the planted triplet's carriers frequent, so its
+    # association clearly beats every permutation's best (checked against the oracle)
+    g, p = O.gen_hwe(95, 600, 36, 300, maf=(0.3, 0.5), planted=[(4, 17, 30)], effects=[0.85])
     R = 64
     reps = _perms(p, R, 7)
     with epik2.Server(0, batch_work=2e9) as srv:
