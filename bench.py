@@ -252,6 +252,9 @@ def run_ours(args, rank, world, local_rank):
     if args.pair_tile:
         ctx.set_pair_tile(args.pair_tile)
         tune = dict(tune, pair_tile=args.pair_tile)
+    if args.overlap:
+        ctx.set_overlap(args.overlap)
+        tune = dict(tune, overlap=1 if args.overlap == 2 else 0)
     engine_tc = tune["engine"] in (epik2.ENGINE_TC, epik2.ENGINE_TC_FP4)
     engine_fp4 = tune["engine"] == epik2.ENGINE_TC_FP4
     flush = torch.empty(args.flush_mb << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
@@ -321,7 +324,7 @@ def run_ours(args, rank, world, local_rank):
     kernel_s = sum(kernel_ms) / 1e3
     achieved_popc = popc_local / kernel_s
     ref_form_popc = sum(step_trip) * words * 27 / kernel_s
-    kernel_name = "k_scan_tc" if engine_tc else "k_scan_int"
+    kernel_name = ("k_scan_pipe" if tune.get("overlap") else "k_scan_tc") if engine_tc else "k_scan_int"
     traffic = None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))[kernel_name]
@@ -442,15 +445,17 @@ def run_ours(args, rank, world, local_rank):
                        "n_cases": info["n_cases"], "step": f"1/{parts} of the triplet space (first-index shard)",
                        "l2": f"flushed before every step ({args.flush_mb} MiB write)",
                        "parallelism": f"{world} GPU(s), shard-parallel",
-                       "engine": ("tensor cores (tcgen05 %s), %d words per stage, %d SNPs j per tile"
+                       "engine": ("tensor cores (tcgen05 %s), %d words per stage, %d SNPs j per tile%s"
                                   % ("block-scaled FP4" if engine_fp4 else "int8", tune["stage_words"],
-                                     tune["pair_tile"])) if engine_tc
-                       else "integer (LOP3+POPC)",
+                                     tune["pair_tile"], ", overlapped scoring" if tune.get("overlap") else ""))
+                       if engine_tc else "integer (LOP3+POPC)",
                        "autotune_rates": {"int": tune["rate_int"], "tc_int8_4": tune["rate_tc4"],
                                           "tc_int8_8": tune["rate_tc8"], "tc_fp4_8_j32": tune["rate_fp4_8"],
                                           "tc_fp4_8_j64": tune["rate_fp4_8_pair"],
                                           "tc_fp4_16_j32": tune["rate_fp4_16_single"],
-                                          "tc_fp4_16_j64": tune["rate_fp4_16"]}},
+                                          "tc_fp4_16_j64": tune["rate_fp4_16"],
+                                          "tc_fp4_4_j64_overlap": tune["rate_fp4_4_overlap"],
+                                          "tc_fp4_8_j64_overlap": tune["rate_fp4_8_overlap"]}},
             "roofline": roof,
             "clocks": clocks,
             "gpu_launches": launches,
@@ -730,6 +735,7 @@ def main():
                     help="plain form: search engine (default: the autotuner's choice)")
     ap.add_argument("--stage-words", type=int, default=0, help="plain form: tensor-core stage depth (0 = tuned)")
     ap.add_argument("--pair-tile", type=int, default=0, help="plain form: SNPs j per tensor-core tile (0 = tuned)")
+    ap.add_argument("--overlap", type=int, default=0, help="plain form: overlapped kernel 0 = tuned, 1 = off, 2 = on")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-drain", type=float, default=30.0)
     ap.add_argument("--no-forms", action="store_true",

@@ -39,6 +39,7 @@ struct epik2_ctx {
   int engine = 0;               // default engine: 0 = auto, 1 = integer, 2 = tensor cores int8, 3 = tensor cores FP4
   int stage_words = 0;          // default tensor-core stage depth: 0 = autotuned
   int pair_tile = 0;            // default tensor-core pair tile: 0 = autotuned, 32 or 64
+  int overlap = 0;              // default overlapped-kernel choice: 0 = tuned, 1 = off, 2 = on
   int scan_blocks = 0;          // integer engine grid
   int tc_blocks = 0;            // tensor-core engine grid (one CTA per SM)
   int n_slots = 0;              // per-warp slots, enough for either grid
@@ -262,49 +263,75 @@ int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
 
 int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_k, int n_warps);
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
-                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair);
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair,
+                bool overlap);
 
 // FP4 accumulators are FP32: counts are exact below 2^24 per class.
 bool fp4_exact(const DevDataset& d) { return d.n_controls < (1 << 24) && d.n_cases < (1 << 24); }
 int tuned(epik2_ctx* ctx, DevDataset& d, epik2_tune* out);
 
-// The tensor-core configurations the autotuner times: format, words per stage, pair tile.
+// The tensor-core configurations the autotuner times: format, words per stage, pair tile,
+// overlapped kernel.
 struct TcConfig {
   int engine, kw;
-  bool pair;
+  bool pair, overlap;
 };
-constexpr TcConfig kTcConfigs[6] = {{EPIK2_ENGINE_TC, 4, false},     {EPIK2_ENGINE_TC, 8, false},
-                                    {EPIK2_ENGINE_TC_FP4, 8, false}, {EPIK2_ENGINE_TC_FP4, 8, true},
-                                    {EPIK2_ENGINE_TC_FP4, 16, false}, {EPIK2_ENGINE_TC_FP4, 16, true}};
+constexpr int kNumTcConfigs = 8;
+constexpr TcConfig kTcConfigs[kNumTcConfigs] = {
+    {EPIK2_ENGINE_TC, 4, false, false},     {EPIK2_ENGINE_TC, 8, false, false},
+    {EPIK2_ENGINE_TC_FP4, 8, false, false}, {EPIK2_ENGINE_TC_FP4, 8, true, false},
+    {EPIK2_ENGINE_TC_FP4, 16, false, false}, {EPIK2_ENGINE_TC_FP4, 16, true, false},
+    {EPIK2_ENGINE_TC_FP4, 4, true, true},   {EPIK2_ENGINE_TC_FP4, 8, true, true}};
 
 // Measured rate of a configuration in a tuner record (0 = not measured).
-double tune_rate(const epik2_tune& t, int engine, int kw, bool pair) {
+double tune_rate(const epik2_tune& t, int engine, int kw, bool pair, bool overlap) {
   if (engine == EPIK2_ENGINE_INT) return t.rate_int;
-  if (engine == EPIK2_ENGINE_TC) return pair ? 0.0 : (kw == 4 ? t.rate_tc4 : t.rate_tc8);
+  if (engine == EPIK2_ENGINE_TC) return (pair || overlap) ? 0.0 : (kw == 4 ? t.rate_tc4 : t.rate_tc8);
+  if (overlap) return !pair ? 0.0 : (kw == 4 ? t.rate_fp4_4_overlap : kw == 8 ? t.rate_fp4_8_overlap : 0.0);
   if (kw == 8) return pair ? t.rate_fp4_8_pair : t.rate_fp4_8;
-  return pair ? t.rate_fp4_16 : t.rate_fp4_16_single;
+  if (kw == 16) return pair ? t.rate_fp4_16 : t.rate_fp4_16_single;
+  return 0.0;
+}
+
+// A configuration the kernels implement.
+bool config_valid(int engine, int kw, bool pair, bool overlap) {
+  if (engine == EPIK2_ENGINE_TC) return (kw == 4 || kw == 8) && !pair && !overlap;
+  if (engine != EPIK2_ENGINE_TC_FP4) return false;
+  if (overlap) return pair && (kw == 4 || kw == 8);
+  return kw == 8 || kw == 16;
+}
+
+// Whether a dataset can take a configuration.
+bool config_fits(const TcConfig& c, bool can_fp4, bool can_overlap) {
+  if (c.engine == EPIK2_ENGINE_TC_FP4 && !can_fp4) return false;
+  return !c.overlap || can_overlap;
 }
 
 // Batched-plan code of a configuration.
-int tc_code(int kw, bool fp4, bool pair) { return kw * 4 + (pair ? 2 : 0) + (fp4 ? 1 : 0); }
+int tc_code(int kw, bool fp4, bool pair, bool overlap) {
+  return kw * 8 + (overlap ? 4 : 0) + (pair ? 2 : 0) + (fp4 ? 1 : 0);
+}
 
 // Fill in the unset parts (0) of a requested configuration: the tuner's choice when it
-// matches what was asked, else the fastest measured configuration that does.
-void complete_config(const epik2_tune& t, bool can_fp4, int& engine, int& kw, int& pt) {
-  if (engine == 0 && kw == 0 && pt == 0 && (t.engine != EPIK2_ENGINE_TC_FP4 || can_fp4)) {
+// matches what was asked, else the fastest measured configuration that does.  ov: 0 =
+// either kernel, 1 = sequential, 2 = overlapped.
+void complete_config(const epik2_tune& t, bool can_fp4, bool can_overlap, int& engine, int& kw, int& pt, int& ov) {
+  if (engine == 0 && kw == 0 && pt == 0 && ov == 0 && (t.engine != EPIK2_ENGINE_TC_FP4 || can_fp4)) {
     engine = t.engine;
     kw = t.stage_words;
     pt = t.pair_tile;
+    ov = t.overlap ? 2 : 1;
     return;
   }
   double best = -1.0;
-  TcConfig pick{engine ? engine : t.engine, kw, pt == 64};
+  TcConfig pick{engine ? engine : t.engine, kw, pt == 64, ov == 2};
   for (const TcConfig& c : kTcConfigs) {
     if (engine && c.engine != engine) continue;
     if (kw && c.kw != kw) continue;
     if (pt && c.pair != (pt == 64)) continue;
-    if (c.engine == EPIK2_ENGINE_TC_FP4 && !can_fp4) continue;
-    const double r = tune_rate(t, c.engine, c.kw, c.pair);
+    if (ov && c.overlap != (ov == 2)) continue;
+    if (!config_fits(c, can_fp4, can_overlap)) continue;
+    const double r = tune_rate(t, c.engine, c.kw, c.pair, c.overlap);
     if (r > best) {
       best = r;
       pick = c;
@@ -313,7 +340,9 @@ void complete_config(const epik2_tune& t, bool can_fp4, int& engine, int& kw, in
   engine = pick.engine;
   kw = pick.kw;
   pt = pick.pair ? 64 : 32;
+  ov = pick.overlap ? 2 : 1;
 }
+
 int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* dump_tables, float* dump_scores,
              BestSlot* best_out);
 
@@ -339,26 +368,33 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   if (opts && opts->engine != 0) engine = opts->engine;
   int kw = (opts && opts->stage_words) ? opts->stage_words : ctx->stage_words;
   int pt = (opts && opts->pair_tile) ? opts->pair_tile : ctx->pair_tile;
+  int ov = (opts && opts->overlap) ? opts->overlap : ctx->overlap;
   if (pt != 0 && pt != 32 && pt != 64) return fail(ctx, EPIK2_E_INVALID, "pair_tile must be 0, 32 or 64");
+  if (ov < 0 || ov > 2) return fail(ctx, EPIK2_E_INVALID, "overlap must be 0, 1 or 2");
   if (engine == EPIK2_ENGINE_TC_FP4 && !fp4_exact(d))
     return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
+  const bool can_overlap = fp4_exact(d) && pipe_fits(d.n_controls, d.n_cases);
+  if (ov == 2 && !can_overlap)
+    return fail(ctx, EPIK2_E_TOO_LARGE, "overlapped kernel: classes of at most 65535 samples");
   if (engine == 0 || ((engine == 2 || engine == 3) && kw == 0)) {
     epik2_tune t{};
     int r = tuned(ctx, d, &t);
     if (r) return r;
-    if (engine == 0) {  // a requested stage depth or pair tile that one format alone takes picks it
-      if (kw == 4) engine = EPIK2_ENGINE_TC;
-      else if (kw == 16 || pt == 64) engine = fp4_exact(d) ? EPIK2_ENGINE_TC_FP4 : EPIK2_ENGINE_TC;
+    if (engine == 0) {  // a requested option that one format alone takes picks that format
+      if (kw == 4 && ov != 2) engine = EPIK2_ENGINE_TC;
+      else if (kw == 16 || pt == 64 || ov == 2) engine = fp4_exact(d) ? EPIK2_ENGINE_TC_FP4 : EPIK2_ENGINE_TC;
     }
-    complete_config(t, fp4_exact(d), engine, kw, pt);
+    complete_config(t, fp4_exact(d), can_overlap, engine, kw, pt, ov);
   }
-  if (pt == 0) pt = (engine == EPIK2_ENGINE_TC_FP4 && kw == 16) ? 64 : 32;  // stage depth given, pair tile not
-  if (engine == 2 && kw != 0 && kw != 4 && kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
-  if (engine == 3 && kw != 0 && kw != 8 && kw != 16)
-    return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 8 or 16 with the FP4 engine");
-  if (engine == 2 && pt == 64) return fail(ctx, EPIK2_E_INVALID, "pair tiles of 64 SNPs run on the FP4 format only");
-  if (engine == 2 || engine == 3)
-    return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts, kw, engine == 3, pt == 64);
+  if (pt == 0) pt = (engine == EPIK2_ENGINE_TC_FP4 && (kw == 16 || ov == 2)) ? 64 : 32;  // not given: by depth
+  if (engine == 2 || engine == 3) {
+    if (!config_valid(engine, kw, pt == 64, ov == 2))
+      return fail(ctx, EPIK2_E_INVALID,
+                  "tensor-core configuration: int8 takes 4 or 8 words per stage on 32-SNP tiles; FP4 takes 8 or 16 "
+                  "(32- or 64-SNP tiles), or 4 or 8 overlapped on 64-SNP tiles");
+    return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts, kw, engine == 3, pt == 64,
+                       ov == 2);
+  }
 
   const int64_t n_first = std::max<int64_t>(ie - ib, 1);
   std::vector<int64_t> off((size_t)n_first + 1, 0);
@@ -521,10 +557,12 @@ int run_pairs_tc(epik2_ctx* ctx, DevDataset& d) {
 // Tensor-core engine: one CTA per SM, tiles = pair blocks (i, j0..j0+31) x k blocks of
 // 128 (int8 format) or 112 (FP4 format) SNPs.
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
-                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair) {
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair,
+                bool overlap) {
   const int64_t m = d.n_snps;
   const int64_t kk = tc_k_per_tile(fp4);
   pair = pair && fp4;
+  overlap = overlap && pair;
   const int64_t jstep = pair ? 64 : 32;  // SNPs j per tile (a CTA pair takes 64)
   const int grid = pair ? tc_pair_blocks(ctx->tc_blocks) : ctx->tc_blocks;
   std::vector<uint32_t> ij;
@@ -591,7 +629,10 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   p.test_withhold = pair ? 0 : ctx->test_withhold;
   if (!pair) ctx->test_withhold = 0;
   CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
-  CK(ctx, launch_scan_tc(p, grid, kw, fp4, pair, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
+  if (overlap)
+    CK(ctx, launch_scan_pipe(p, grid, kw, dump_tables != nullptr, ctx->stream), "overlapped tensor-core kernel");
+  else
+    CK(ctx, launch_scan_tc(p, grid, kw, fp4, pair, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
   CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
   const int n_warps = grid * tc_warps_per_block();
   CK(ctx, launch_reduce_best(ctx->d_slots, n_warps, ctx->d_best, ctx->stream), "reduce kernel");
@@ -634,18 +675,22 @@ int autotune_now(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
   while (ie < m && (triplets_before(m, ie) * 64 < total || triplets_before(m, ie) < 4ll * ctx->tc_blocks * 4096)) ie++;
   const double ts = (double)triplets_before(m, ie) * (double)d.n_samples;
   // candidates: integer; int8 tensor cores, 4 or 8 words per stage (pair tile 32); FP4 tensor
-  // cores, 8 or 16 words per stage, pair tile 32 (one CTA) or 64 (CTA pairs)
-  constexpr int kCand = 7;
-  double rate[kCand] = {0, 0, 0, 0, 0, 0, 0};
-  const int n_cand = fp4_exact(d) ? kCand : 3;
-  for (int c = 0; c < n_cand; c++) {
+  // cores, 8 or 16 words per stage, pair tile 32 (one CTA) or 64 (CTA pairs); the overlapped
+  // FP4 CTA-pair kernel at 4 and 8 words per stage
+  constexpr int kCand = 1 + kNumTcConfigs;
+  double rate[kCand] = {};
+  const bool can_fp4 = fp4_exact(d), can_overlap = can_fp4 && pipe_fits(d.n_controls, d.n_cases);
+  for (int c = 0; c < kCand; c++) {
     epik2_opts o{};
     if (c == 0) {
       o.engine = EPIK2_ENGINE_INT;
     } else {
-      o.engine = kTcConfigs[c - 1].engine;
-      o.stage_words = kTcConfigs[c - 1].kw;
-      o.pair_tile = kTcConfigs[c - 1].pair ? 64 : 32;
+      const TcConfig& tc = kTcConfigs[c - 1];
+      if (!config_fits(tc, can_fp4, can_overlap)) continue;
+      o.engine = tc.engine;
+      o.stage_words = tc.kw;
+      o.pair_tile = tc.pair ? 64 : 32;
+      o.overlap = tc.overlap ? 2 : 1;
     }
     o.snp_begin = 0;
     o.snp_end = ie;
@@ -664,17 +709,21 @@ int autotune_now(epik2_ctx* ctx, DevDataset& d, epik2_tune* out) {
   t.rate_fp4_8_pair = rate[4];
   t.rate_fp4_16_single = rate[5];
   t.rate_fp4_16 = rate[6];
+  t.rate_fp4_4_overlap = rate[7];
+  t.rate_fp4_8_overlap = rate[8];
   int best = 0;
-  for (int c = 1; c < n_cand; c++)
+  for (int c = 1; c < kCand; c++)
     if (rate[c] > rate[best]) best = c;
   if (best == 0) {  // the integer engine; the stage depth is the faster int8 one
     t.engine = EPIK2_ENGINE_INT;
     t.stage_words = rate[2] > rate[1] ? 8 : 4;
     t.pair_tile = 32;
+    t.overlap = 0;
   } else {
     t.engine = kTcConfigs[best - 1].engine;
     t.stage_words = kTcConfigs[best - 1].kw;
     t.pair_tile = kTcConfigs[best - 1].pair ? 64 : 32;
+    t.overlap = kTcConfigs[best - 1].overlap ? 1 : 0;
   }
   *out = t;
   return EPIK2_OK;
@@ -757,7 +806,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     for (int32_t b = 0; b < n; b++) {
       const bool fp4 = codes[b] & 1;
       const int64_t m = ds[b]->n_snps, kk = tc_k_per_tile(fp4);
-      const int64_t jstep = (codes[b] & 2) ? 64 : 32;
+      const int64_t jstep = (codes[b] & 2) ? 64 : 32;  // CTA pairs (both kernels)
       auto li = lists.find({m, kk * 2 + (jstep == 64 ? 1 : 0)});
       if (li == lists.end()) {
         ListInfo L{(int64_t)pb_off_all.size(), (int64_t)pb_ij_all.size(), 0, 0};
@@ -824,6 +873,7 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
     // capture: reset slots, counters and error word; one batched search per group;
     // per-dataset reduce; optional FP64 rescore; read back
     CK(ctx, tc_configure(), "configure");
+    CK(ctx, pipe_configure(), "configure");
     CK(ctx, launch_fill_slots(pl->d_job_slots, (int64_t)n * grid, ctx->stream), "configure");  // also loads modules
     CK(ctx, cudaStreamSynchronize(ctx->stream), "configure");
     CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
@@ -843,9 +893,12 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
       p.n_jobs = n;
       p.job_slots = pl->d_job_slots;
       p.n_tiles = nt;
-      const bool gp = (group_code[g] & 2) != 0;
-      e = launch_scan_tc(p, gp ? tc_pair_blocks(grid) : grid, group_code[g] >> 2, group_code[g] & 1, gp, false,
-                         ctx->stream);
+      const bool gp = (group_code[g] & 2) != 0, gov = (group_code[g] & 4) != 0;
+      if (gov)
+        e = launch_scan_pipe(p, tc_pair_blocks(grid), group_code[g] >> 3, false, ctx->stream);
+      else
+        e = launch_scan_tc(p, gp ? tc_pair_blocks(grid) : grid, group_code[g] >> 3, group_code[g] & 1, gp, false,
+                           ctx->stream);
     }
     if (e == cudaSuccess) e = launch_reduce_jobs(pl->d_job_slots, n, grid, pl->d_results, ctx->stream);
     if (e == cudaSuccess && rescore) e = launch_rescore_jobs(pl->d_jobs, pl->d_results, n, pl->d_resc, ctx->stream);
@@ -1033,6 +1086,13 @@ int epik2_set_wait_limit(epik2_ctx* ctx, int64_t sm_clocks) {
 int epik2_test_withhold_arrival(epik2_ctx* ctx) {
   if (!ctx) return EPIK2_E_INVALID;
   ctx->test_withhold = 1;
+  return EPIK2_OK;
+}
+
+int epik2_set_overlap(epik2_ctx* ctx, int overlap) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (overlap < 0 || overlap > 2) return fail(ctx, EPIK2_E_INVALID, "overlap must be 0, 1 or 2");
+  ctx->overlap = overlap;
   return EPIK2_OK;
 }
 
@@ -1350,20 +1410,30 @@ int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, cons
   const int engine_req = opts ? opts->engine : 0;
   const int kw_req = opts ? opts->stage_words : 0;
   const int pt_req = opts ? opts->pair_tile : 0;
+  const int ov_req = opts ? opts->overlap : 0;
   if (engine_req == EPIK2_ENGINE_INT) return fail(ctx, EPIK2_E_INVALID, "the batched form runs on the tensor cores");
   if (engine_req < 0 || engine_req > EPIK2_ENGINE_TC_FP4) return fail(ctx, EPIK2_E_INVALID, "unknown engine");
   if (pt_req != 0 && pt_req != 32 && pt_req != 64) return fail(ctx, EPIK2_E_INVALID, "pair_tile must be 0, 32 or 64");
-  bool all_fp4 = true;
-  for (DevDataset* d : ds) all_fp4 = all_fp4 && fp4_exact(*d);
+  if (ov_req < 0 || ov_req > 2) return fail(ctx, EPIK2_E_INVALID, "overlap must be 0, 1 or 2");
+  bool all_fp4 = true, all_overlap = true;
+  for (DevDataset* d : ds) {
+    all_fp4 = all_fp4 && fp4_exact(*d);
+    all_overlap = all_overlap && fp4_exact(*d) && pipe_fits(d->n_controls, d->n_cases);
+  }
   if (engine_req == EPIK2_ENGINE_TC_FP4 && !all_fp4)
     return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
-  TcConfig pick{0, 0, false};
+  if (ov_req == 2 && !all_overlap)
+    return fail(ctx, EPIK2_E_TOO_LARGE, "overlapped kernel: classes of at most 65535 samples");
+  TcConfig pick{0, 0, false, false};
   bool have = false;
-  if (engine_req != 0 && kw_req != 0 && (pt_req != 0 || engine_req == EPIK2_ENGINE_TC)) {
-    pick = TcConfig{engine_req, kw_req, pt_req == 64};
+  if (engine_req != 0 && kw_req != 0 && (pt_req != 0 || engine_req == EPIK2_ENGINE_TC) && ov_req != 0) {
+    pick = TcConfig{engine_req, kw_req, pt_req == 64, ov_req == 2};
     have = true;
-  } else if (engine_req == EPIK2_ENGINE_TC_FP4 && kw_req != 0 && pt_req == 0) {
-    pick = TcConfig{engine_req, kw_req, kw_req == 16};  // stage depth given, pair tile not
+  } else if (engine_req == EPIK2_ENGINE_TC && kw_req != 0) {
+    pick = TcConfig{engine_req, kw_req, false, false};
+    have = true;
+  } else if (engine_req == EPIK2_ENGINE_TC_FP4 && kw_req != 0 && pt_req == 0 && ov_req == 0) {
+    pick = TcConfig{engine_req, kw_req, kw_req == 16, false};  // stage depth given, nothing else
     have = true;
   } else {
     std::vector<epik2_tune> tunes;
@@ -1378,11 +1448,12 @@ int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, cons
       if (engine_req && c.engine != engine_req) continue;
       if (kw_req && c.kw != kw_req) continue;
       if (pt_req && c.pair != (pt_req == 64)) continue;
-      if (c.engine == EPIK2_ENGINE_TC_FP4 && !all_fp4) continue;
+      if (ov_req && c.overlap != (ov_req == 2)) continue;
+      if (!config_fits(c, all_fp4, all_overlap)) continue;
       double time = 0.0;
       bool ok = true;
       for (size_t b = 0; b < ds.size() && ok; b++) {
-        const double rate = tune_rate(tunes[b], c.engine, c.kw, c.pair);
+        const double rate = tune_rate(tunes[b], c.engine, c.kw, c.pair, c.overlap);
         const double m = (double)ds[b]->n_snps;
         ok = rate > 0.0;
         time += m * (m - 1) * (m - 2) / 6.0 * (double)ds[b]->n_samples / (ok ? rate : 1.0);
@@ -1396,11 +1467,11 @@ int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, cons
   }
   if (!have) return fail(ctx, EPIK2_E_INVALID, "no tensor-core configuration matches the request");
   const bool fp4 = pick.engine == EPIK2_ENGINE_TC_FP4;
-  if (!fp4 && pick.kw != 4 && pick.kw != 8) return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 4 or 8");
-  if (fp4 && pick.kw != 8 && pick.kw != 16)
-    return fail(ctx, EPIK2_E_INVALID, "stage_words must be 0, 8 or 16 with the FP4 engine");
-  if (!fp4 && pick.pair) return fail(ctx, EPIK2_E_INVALID, "pair tiles of 64 SNPs run on the FP4 format only");
-  const std::vector<int> codes(ds.size(), tc_code(pick.kw, fp4, pick.pair && fp4));
+  if (!config_valid(pick.engine, pick.kw, pick.pair, pick.overlap))
+    return fail(ctx, EPIK2_E_INVALID,
+                "tensor-core configuration: int8 takes 4 or 8 words per stage on 32-SNP tiles; FP4 takes 8 or 16 "
+                "(32- or 64-SNP tiles), or 4 or 8 overlapped on 64-SNP tiles");
+  const std::vector<int> codes(ds.size(), tc_code(pick.kw, fp4, pick.pair && fp4, pick.overlap));
   return run_batch(ctx, ds, ids, codes, opts && opts->rescore_fp64, out);
 }
 

@@ -156,6 +156,11 @@ int scan_blocks_per_sm();
 cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool pair, bool dump,
                            cudaStream_t stream);
 int tc_k_per_tile(bool fp4);  // SNPs k per tensor-core tile: 128 (int8) or 112 (FP4)
+// The overlapped FP4 CTA-pair kernel (scan_pipe.cu): scoring of a tile runs while the next
+// tile counts; 4 or 8 words per stage; classes of at most 65535 samples (16-bit staging).
+cudaError_t launch_scan_pipe(const TcParams& p, int blocks, int words_per_stage, bool dump, cudaStream_t stream);
+bool pipe_fits(int64_t n_controls, int64_t n_cases);
+cudaError_t pipe_configure();  // dynamic shared-memory limits of the overlapped kernels (once)
 int tc_pair_blocks(int sms);  // resident CTAs of the CTA-pair kernel (even)
 // Tile descriptors of one pair-block list (prefix sums pb_off[0..n_pb], (i, j0) pairs) into
 // out[pb_off[b] ...], tagged with `job`.

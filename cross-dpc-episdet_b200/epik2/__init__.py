@@ -68,7 +68,8 @@ class Tune(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("rate_int", ctypes.c_double),
                 ("rate_tc4", ctypes.c_double), ("rate_tc8", ctypes.c_double), ("rate_fp4_8", ctypes.c_double),
                 ("rate_fp4_16", ctypes.c_double), ("rate_fp4_8_pair", ctypes.c_double),
-                ("rate_fp4_16_single", ctypes.c_double), ("pair_tile", ctypes.c_int32), ("_pad", ctypes.c_int32)]
+                ("rate_fp4_16_single", ctypes.c_double), ("pair_tile", ctypes.c_int32), ("overlap", ctypes.c_int32),
+                ("rate_fp4_4_overlap", ctypes.c_double), ("rate_fp4_8_overlap", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -91,7 +92,7 @@ class ServerStats(ctypes.Structure):
 
 class Opts(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("top_k", ctypes.c_int32), ("rescore_fp64", ctypes.c_int32),
-                ("pair_tile", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("pair_tile", ctypes.c_int32), ("stage_words", ctypes.c_int32), ("overlap", ctypes.c_int32),
                 ("snp_begin", ctypes.c_int64), ("snp_end", ctypes.c_int64)]
 
 
@@ -150,6 +151,7 @@ def library():
         "epik2_set_stage_words": ([p, ctypes.c_int], ctypes.c_int),
         "epik2_set_wait_limit": ([p, i64], ctypes.c_int),
         "epik2_set_pair_tile": ([p, ctypes.c_int], ctypes.c_int),
+        "epik2_set_overlap": ([p, ctypes.c_int], ctypes.c_int),
         "epik2_test_withhold_arrival": ([p], ctypes.c_int),
         "epik2_plink_dims": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
                              ctypes.c_int),
@@ -268,7 +270,7 @@ def n_triplets(m):
 class Context:
     """One device context: owns a CUDA stream and the resident datasets."""
 
-    def __init__(self, device=0, engine=ENGINE_AUTO, stage_words=0, pair_tile=0):
+    def __init__(self, device=0, engine=ENGINE_AUTO, stage_words=0, pair_tile=0, overlap=0):
         self._lib = library()
         h = ctypes.c_void_p()
         r = self._lib.epik2_create(ctypes.byref(h), device)
@@ -281,6 +283,8 @@ class Context:
             self.set_stage_words(stage_words)
         if pair_tile:
             self.set_pair_tile(pair_tile)
+        if overlap:
+            self.set_overlap(overlap)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -319,6 +323,10 @@ class Context:
     def set_pair_tile(self, pair_tile):
         """Default tensor-core pair tile (0 = autotuned; 32, or 64 = FP4 on CTA pairs)."""
         self._check(self._lib.epik2_set_pair_tile(self._h, pair_tile))
+
+    def set_overlap(self, overlap):
+        """Default overlapped-kernel choice (0 = tuned, 1 = off, 2 = on; FP4 on CTA pairs)."""
+        self._check(self._lib.epik2_set_overlap(self._h, overlap))
 
     def set_wait_limit(self, sm_clocks):
         """SM clocks a bounded device-side wait lasts before the search gives up (0 = ~2 s)."""

@@ -78,7 +78,9 @@ typedef struct {
                           pair_tile 0: 64 for FP4 at 16 words, else 32) */
   int32_t stage_words;  /* tuning, tensor cores: 32-sample words per pipeline stage, 4 or 8 (int8),
                            8 or 16 (FP4); 0 = autotuned */
-  int32_t reserved;    /* must be 0 */
+  int32_t overlap;     /* tuning, FP4 on CTA pairs: 2 = the overlapped kernel (a tile's scoring runs
+                          while the next tile counts; 4 or 8 words per stage; classes of at most
+                          65535 samples), 1 = the sequential one, 0 = tuned */
   int64_t snp_begin;   /* restrict the first index i to [snp_begin, snp_end); 0,0 = all */
   int64_t snp_end;
 } epik2_opts;
@@ -111,6 +113,8 @@ int epik2_set_stage_words(epik2_ctx *ctx, int stage_words);
 /* Default tensor-core pair tile of the context (used when epik2_opts.pair_tile is 0): 0 =
  * autotuned, 32 or 64 (64 = FP4 on clusters of two CTAs). */
 int epik2_set_pair_tile(epik2_ctx *ctx, int pair_tile);
+/* Default of epik2_opts.overlap for the context: 0 = tuned, 1 = off, 2 = on. */
+int epik2_set_overlap(epik2_ctx *ctx, int overlap);
 
 /* Run the context's work on a caller-owned stream (e.g. a PyTorch stream); NULL restores
  * the context's own stream.  The library still synchronises that stream before it
@@ -232,11 +236,12 @@ int epik2_scan_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int
 int epik2_scan_batch(epik2_ctx *ctx, const int32_t *dataset_ids, int32_t n, const epik2_opts *opts,
                      epik2_best *out);
 
-/* Autotuner (no reference counterpart).  Times seven configurations on a slice of the
+/* Autotuner (no reference counterpart).  Times nine configurations on a slice of the
  * dataset (about 1/64 of its triplets, at least a few tiles per SM): the integer engine; the
  * int8 tensor-core engine at 4 and 8 words (128 and 256 samples) per stage; and, when its
  * accumulators are exact for the dataset, the FP4 tensor-core engine at 8 and 16 words per
- * stage, each with a pair tile of 32 SNPs j (one CTA) and of 64 (a cluster of two CTAs).
+ * stage, each with a pair tile of 32 SNPs j (one CTA) and of 64 (a cluster of two CTAs), and
+ * the overlapped FP4 CTA-pair kernel at 4 and 8 words per stage (classes <= 65535 samples).
  * Caches the fastest per shape bucket (log2 of samples and SNPs); EPIK2_ENGINE_AUTO scans and
  * the batched form use the cached rates.  Reports the choice and the measured rates
  * (triplet*samples/s; 0 = not a candidate).  The k-strip (SNPs k per tile: 128 int8, 112
@@ -253,7 +258,9 @@ typedef struct {
   double rate_fp4_8_pair;    /* FP4, 8 words, 64 j (CTA pairs) */
   double rate_fp4_16_single; /* FP4, 16 words, 32 j */
   int32_t pair_tile;     /* pair tile chosen: 32 or 64 SNPs j */
-  int32_t _pad;
+  int32_t overlap;       /* 1 = the overlapped kernel was chosen */
+  double rate_fp4_4_overlap; /* overlapped FP4 CTA-pair kernel, 4 words per stage */
+  double rate_fp4_8_overlap; /* the same, 8 words per stage */
 } epik2_tune;
 int epik2_autotune(epik2_ctx *ctx, int32_t dataset_id, epik2_tune *out);
 

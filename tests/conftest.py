@@ -59,14 +59,20 @@ def pytest_collection_modifyitems(config, items):
 ENGINES = {1: "int", 2: "tc", 3: "fp4"}
 
 
-@pytest.fixture(scope="session", params=[(1, 0, 0), (2, 0, 0), (3, 8, 32), (3, 16, 64), (3, 8, 64), (3, 16, 32)],
-                ids=["int", "tc", "fp4", "fp4pair", "fp4pair8", "fp4w16"])
+@pytest.fixture(scope="session", params=[(1, 0, 0, 0), (2, 0, 0, 0), (3, 8, 32, 1), (3, 16, 64, 1), (3, 8, 64, 1),
+                                        (3, 16, 32, 1), (3, 4, 64, 2), (3, 8, 64, 2)],
+                ids=["int", "tc", "fp4", "fp4pair", "fp4pair8", "fp4w16", "fp4ov4", "fp4ov8"])
 def ctx(request):
     """A device context per search engine: integer pipe; int8 tensor cores; FP4 tensor cores
     on single CTAs (32 SNPs j per tile) at 8 and 16 words per stage; FP4 on CTA pairs (64 SNPs
-    j per tile) at 16 and 8 words per stage.  Every test that takes `ctx` runs on all six."""
+    j per tile) at 16 and 8 words per stage; the overlapped FP4 CTA-pair kernel at 4 and 8
+    words per stage.  Every test that takes `ctx` runs on all eight.  A configuration a
+    dataset cannot take (the overlapped kernel for classes above 65535 samples) is refused with
+    EPIK2_E_TOO_LARGE."""
     import epik2
-    c = epik2.Context(0, engine=request.param[0], stage_words=request.param[1], pair_tile=request.param[2])
+    c = epik2.Context(0, engine=request.param[0], stage_words=request.param[1], pair_tile=request.param[2],
+                      overlap=request.param[3])
+    c.config = request.param
     yield c
     c.close()
 

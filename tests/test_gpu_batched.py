@@ -16,12 +16,14 @@ MIXED = [  # (seed, samples, SNPs, cases): uneven sizes, class splits and tile c
 ]
 
 
-@pytest.mark.parametrize("engine,stage_words,pair_tile", [(2, 4, 32), (2, 8, 32), (3, 8, 32), (3, 16, 64), (3, 8, 64),
-                                                          (3, 16, 32)],
-                         ids=["tc-4", "tc-8", "fp4-8", "fp4-16-pair", "fp4-8-pair", "fp4-16"])
-def test_batch_equals_separate_runs_and_oracle(engine, stage_words, pair_tile):
+@pytest.mark.parametrize("engine,stage_words,pair_tile,overlap",
+                         [(2, 4, 32, 1), (2, 8, 32, 1), (3, 8, 32, 1), (3, 16, 64, 1), (3, 8, 64, 1), (3, 16, 32, 1),
+                          (3, 4, 64, 2), (3, 8, 64, 2)],
+                         ids=["tc-4", "tc-8", "fp4-8", "fp4-16-pair", "fp4-8-pair", "fp4-16", "fp4-4-overlap",
+                              "fp4-8-overlap"])
+def test_batch_equals_separate_runs_and_oracle(engine, stage_words, pair_tile, overlap):
     data = [O.gen_hwe(sd, S, M, c) for sd, S, M, c in MIXED]
-    kw = dict(engine=engine, stage_words=stage_words, pair_tile=pair_tile)
+    kw = dict(engine=engine, stage_words=stage_words, pair_tile=pair_tile, overlap=overlap)
     with epik2.Context(0) as ctx:
         ids = [ctx.load(g, p) for g, p in data]
         batched = ctx.scan_batch(ids, **kw)
@@ -75,12 +77,14 @@ def test_autotune_reports_all_candidates():
     assert t["stage_words"] in ((8, 16) if t["engine"] == epik2.ENGINE_TC_FP4 else (4, 8))
     assert t["pair_tile"] in ((32, 64) if t["engine"] == epik2.ENGINE_TC_FP4 else (32,))
     assert min(t["rate_int"], t["rate_tc4"], t["rate_tc8"], t["rate_fp4_8"], t["rate_fp4_16"], t["rate_fp4_8_pair"],
-               t["rate_fp4_16_single"]) > 0
-    rates = {(epik2.ENGINE_INT, 0, 32): t["rate_int"], (epik2.ENGINE_TC, 4, 32): t["rate_tc4"],
-             (epik2.ENGINE_TC, 8, 32): t["rate_tc8"], (epik2.ENGINE_TC_FP4, 8, 32): t["rate_fp4_8"],
-             (epik2.ENGINE_TC_FP4, 8, 64): t["rate_fp4_8_pair"], (epik2.ENGINE_TC_FP4, 16, 32): t["rate_fp4_16_single"],
-             (epik2.ENGINE_TC_FP4, 16, 64): t["rate_fp4_16"]}
-    chosen = (t["engine"], 0 if t["engine"] == epik2.ENGINE_INT else t["stage_words"], t["pair_tile"])
+               t["rate_fp4_16_single"], t["rate_fp4_4_overlap"], t["rate_fp4_8_overlap"]) > 0
+    rates = {(epik2.ENGINE_INT, 0, 32, 0): t["rate_int"], (epik2.ENGINE_TC, 4, 32, 0): t["rate_tc4"],
+             (epik2.ENGINE_TC, 8, 32, 0): t["rate_tc8"], (epik2.ENGINE_TC_FP4, 8, 32, 0): t["rate_fp4_8"],
+             (epik2.ENGINE_TC_FP4, 8, 64, 0): t["rate_fp4_8_pair"],
+             (epik2.ENGINE_TC_FP4, 16, 32, 0): t["rate_fp4_16_single"],
+             (epik2.ENGINE_TC_FP4, 16, 64, 0): t["rate_fp4_16"], (epik2.ENGINE_TC_FP4, 4, 64, 1): t["rate_fp4_4_overlap"],
+             (epik2.ENGINE_TC_FP4, 8, 64, 1): t["rate_fp4_8_overlap"]}
+    chosen = (t["engine"], 0 if t["engine"] == epik2.ENGINE_INT else t["stage_words"], t["pair_tile"], t["overlap"])
     assert rates[chosen] == max(rates.values())
     r = O.scan(g, p)
     assert b.ijk == r["ijk"]
