@@ -567,8 +567,14 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   const int grid = pair ? tc_pair_blocks(ctx->tc_blocks) : ctx->tc_blocks;
   std::vector<uint32_t> ij;
   std::vector<int64_t> off(1, 0);
-  for (int64_t i = ib; i < ie; i++)
-    for (int64_t j0 = i + 1; j0 <= m - 2; j0 += jstep) {
+  // Pair blocks in the order (u, i) with j0 = i + 1 + jstep*u: consecutive pair blocks (and
+  // the CTAs working on them at the same time) cover nearly the same SNPs j and k, so the
+  // (j, k) pair margins and the k planes they read are shared through L2 instead of being
+  // swept from HBM once per first index.
+  for (int64_t u = 0; ib + 1 + jstep * u <= m - 2; u++)
+    for (int64_t i = ib; i < ie; i++) {
+      const int64_t j0 = i + 1 + jstep * u;
+      if (j0 > m - 2) break;
       ij.push_back((uint32_t)i);
       ij.push_back((uint32_t)j0);
       off.push_back(off.back() + tiles_of_pair_block(j0, m, kk));
@@ -811,8 +817,10 @@ int run_batch(epik2_ctx* ctx, const std::vector<DevDataset*>& ds, const std::vec
       if (li == lists.end()) {
         ListInfo L{(int64_t)pb_off_all.size(), (int64_t)pb_ij_all.size(), 0, 0};
         pb_off_all.push_back(0);
-        for (int64_t i = 0; i < m; i++)
-          for (int64_t j0 = i + 1; j0 <= m - 2; j0 += jstep) {
+        for (int64_t u = 0; 1 + jstep * u <= m - 2; u++)  // (u, i) order, as in run_scan_tc
+          for (int64_t i = 0; i < m; i++) {
+            const int64_t j0 = i + 1 + jstep * u;
+            if (j0 > m - 2) break;
             pb_ij_all.push_back((uint32_t)i);
             pb_ij_all.push_back((uint32_t)j0);
             L.tiles += tiles_of_pair_block(j0, m, kk);
