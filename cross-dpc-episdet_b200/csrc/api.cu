@@ -51,8 +51,6 @@ struct epik2_ctx {
   int64_t pb_cap = 0;
   uint64_t* d_tiles = nullptr;  // tensor-core tile descriptors
   int64_t tiles_cap = 0;
-  uint4* d_bexp = nullptr;      // expanded operand-B rows of the CTA-pair search (16-byte rows)
-  int64_t bexp_cap = 0;
   unsigned long long* d_counter = nullptr;
   BestSlot* d_slots = nullptr;  // one per warp of the scan grid
   BestSlot* d_best = nullptr;
@@ -250,52 +248,6 @@ int ensure_tiles(epik2_ctx* ctx, int64_t n) {
   CK(ctx, cudaMalloc(&ctx->d_tiles, (size_t)n * 8), "alloc tile descriptors");
   ctx->tiles_cap = n;
   return EPIK2_OK;
-}
-
-int ensure_bexp(epik2_ctx* ctx, int64_t n) {
-  if (n <= ctx->bexp_cap) return EPIK2_OK;
-  n = std::max(n, 2 * ctx->bexp_cap);
-  cudaFree(ctx->d_bexp);
-  ctx->d_bexp = nullptr;
-  ctx->bexp_cap = 0;
-  CK(ctx, cudaMalloc(&ctx->d_bexp, (size_t)n * 16), "alloc expanded operand B");
-  ctx->bexp_cap = n;
-  return EPIK2_OK;
-}
-
-// cuTensorMapEncodeTiled from the driver (the library links the static runtime only).
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_tiled_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)f;
-    cudaGetLastError();
-  }
-  return fn;
-}
-
-// Tensor map of the expanded operand B: dims (innermost first) 16 bytes, SNPs (m_pad), padded
-// words, g_k; boxes of 16 bytes x 8 SNPs x 16 words x 1 (one core-matrix group of 8 rows for
-// one stage).  Rows past m_pad read as zeros.
-bool encode_bexp_map(CUtensorMap* map, const uint4* base, int64_t m_pad, int64_t words) {
-  EncodeTiledFn fn = encode_tiled_fn();
-  if (!fn) return false;
-  const cuuint64_t dims[4] = {16, (cuuint64_t)m_pad, (cuuint64_t)words, 2};
-  const cuuint64_t strides[3] = {16, (cuuint64_t)(16 * m_pad), (cuuint64_t)(16 * m_pad * words)};
-  const cuuint32_t box[4] = {16, 8, 16, 1};
-  const cuuint32_t estr[4] = {1, 1, 1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, (void*)base, dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
@@ -682,17 +634,6 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   p.wait_limit = ctx->wait_limit;
   p.test_withhold = pair ? 0 : ctx->test_withhold;
   if (!pair) ctx->test_withhold = 0;
-  if (pair && !overlap && kw == 16) {  // operand B by the tensor-memory accelerator
-    const int64_t p0 = (d.w0 + 15) / 16 * 16, p1 = (d.w1 + 15) / 16 * 16;
-    int rb = ensure_bexp(ctx, 2 * (p0 + p1) * d.m_pad);
-    if (rb) return rb;
-    CK(ctx, launch_expand_b(d.planes, d.m_pad, d.w0, d.w1, p0, p1, ctx->d_bexp, ctx->stream), "expand operand B");
-    ctx->stats.kernel_launches += 1;
-    if (!encode_bexp_map(&p.bexp_map, ctx->d_bexp, d.m_pad, p0 + p1))
-      return fail(ctx, EPIK2_E_CUDA, "tensor map of the expanded operand B");
-    p.use_bexp = 1;
-    p.bexp_p0 = (int32_t)p0;
-  }
   CK(ctx, cudaEventRecord(ctx->ev_start, ctx->stream), "event");
   if (overlap)
     CK(ctx, launch_scan_pipe(p, grid, kw, dump_tables != nullptr, ctx->stream), "overlapped tensor-core kernel");
@@ -1099,7 +1040,6 @@ void epik2_destroy(epik2_ctx* ctx) {
   cudaFree(ctx->d_pb_off);
   cudaFree(ctx->d_pb_ij);
   cudaFree(ctx->d_tiles);
-  cudaFree(ctx->d_bexp);
   cudaFreeHost(ctx->h_best);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);

@@ -1,7 +1,6 @@
 // Internal declarations shared by the host API and the CUDA kernels.
 #pragma once
 #include <cstdint>
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace epik2 {
@@ -139,13 +138,6 @@ struct TcParams {
   long long wait_limit;
   // test hook: CTA 0 withholds one arrival so that its first wait expires (single CTAs)
   int32_t test_withhold;
-  // CTA-pair FP4 search at 16 words per stage (not batched): operand B comes from a copy of
-  // the k SNPs' E2M1 rows expanded once per search (layout [g_k][padded word][SNP][16 bytes],
-  // each class's words padded to a multiple of 16) and is loaded by the tensor-memory
-  // accelerator; bexp_p0 = class 0's padded word count
-  int32_t use_bexp;
-  int32_t bexp_p0;
-  CUtensorMap bexp_map;
 };
 
 // Kernel launchers (scan_int.cu / scan_tc.cu / encode.cu); all asynchronous on `stream`.
@@ -153,10 +145,6 @@ cudaError_t launch_encode(const DevDataset& d, cudaStream_t stream);
 cudaError_t launch_counts(const DevDataset& d, cudaStream_t stream, bool pairs = true);
 // pair margins on tensor cores (the CTA-pair FP4 kernel; exact for classes below 2^24)
 cudaError_t launch_pairs_tc(const TcParams& p, int blocks, cudaStream_t stream);
-// Expanded operand-B copy for the CTA-pair FP4 search (see TcParams::use_bexp): out holds
-// 2 x (p0 + p1) x m_pad rows of 16 bytes, p0/p1 = class words rounded up to 16.
-cudaError_t launch_expand_b(const uint2* planes, int64_t m_pad, int64_t w0, int64_t w1, int64_t p0, int64_t p1,
-                            uint4* out, cudaStream_t stream);
 cudaError_t launch_scan_int(const ScanParams& p, int blocks, bool dump, cudaStream_t stream);
 cudaError_t launch_reduce_best(const BestSlot* slots, int n, BestSlot* out, cudaStream_t stream);
 cudaError_t launch_tables(const DevDataset& d, const uint32_t* triplets, int64_t n, uint32_t* out,

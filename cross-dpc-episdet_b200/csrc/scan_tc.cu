@@ -78,16 +78,10 @@ struct JobView {
 // kMarg (CTA pairs only): the pair-margin form.  Operand A's g_i = 0 rows are all ones and
 // its g_i = 1 rows zero, so D[(j, 0, b)][(k, c)] is the count of (g_j = b, g_k = c): tiles
 // (0, j0, k block) write the pair margins of every j < k < m_pad instead of scoring.
-// kTmaB (CTA pairs, 16 words per stage, not batched): operand B is not expanded by the threads
-// but loaded per stage by the tensor-memory accelerator from the search's expanded copy
-// (p.bexp_map): 14 boxes of 8 SNPs x 16 words (2 KiB, one 8-row core-matrix group each) per
-// CTA, whose bytes complete on the stage's "full" barrier.
-template <int kW, bool kFp4, bool kPair, bool kBatched, bool kDump, bool kTopK, bool kMarg = false,
-          bool kTmaB = false>
-__global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const __grid_constant__ TcParams p) {
+template <int kW, bool kFp4, bool kPair, bool kBatched, bool kDump, bool kTopK, bool kMarg = false>
+__global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) {
   static_assert(!kPair || kFp4, "CTA pairs use the FP4 format");
   static_assert(!kMarg || (kPair && !kBatched && !kDump && !kTopK), "pair margins: plain CTA-pair kernel");
-  static_assert(!kTmaB || (kPair && kW == 16 && !kBatched && !kMarg), "TMA operand B: plain CTA-pair kernel");
   constexpr int kK = kFp4 ? 112 : 128;                // SNPs k per tile -> 2*kK rows of B
   constexpr int kRowBytes = (kFp4 ? 16 : 32) * kW;    // operand bytes per row per stage
   constexpr int kBRows = kPair ? kK : 2 * kK;         // B rows held by this CTA
@@ -299,8 +293,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const __grid_const
 #pragma unroll
         for (int r = 0; r < kW / 8; r++) {
           const int w = p_wbase + 8 * r;
-          if (!kTmaB && kW * c_in + w < wcls && p_on && p_k < m_pad)
-            gk[r] = __ldg(jv.planes + (wb + w) * m_pad + p_k);
+          if (kW * c_in + w < wcls && p_on && p_k < m_pad) gk[r] = __ldg(jv.planes + (wb + w) * m_pad + p_k);
         }
       } else {
 #pragma unroll
@@ -326,20 +319,6 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const __grid_const
         if (__any_sync(kFull, late)) *abort_flag = 1;
         if (__shfl_sync(kFull, *abort_flag, 0)) break;  // warp-uniform
         const uint32_t sA = stage0 + s * kStageBytes, sB = sA + kStageA;
-        if constexpr (kTmaB) {  // this CTA's B rows of the stage: (g_k, 8-SNP group) boxes
-          if (warp == 0 && lane == 0) {
-            const bool c1 = cc >= nc0;
-            const int word = (c1 ? p.bexp_p0 : 0) + kW * (c1 ? cc - nc0 : cc);
-            const int snp0 = k0 + (kK / 2) * (int)crank;
-            bar_expect_tx(bar_full0 + 8 * s, (uint32_t)(2 * (kK / 16) * kSbo));
-#pragma unroll
-            for (int c = 0; c < 2; c++)
-#pragma unroll
-              for (int gq = 0; gq < kK / 16; gq++)
-                tma_load_4d(sB + (uint32_t)((kK / 16) * c + gq) * kSbo, &p.bexp_map, 0, snp0 + 8 * gq, word, c,
-                            bar_full0 + 8 * s);
-          }
-        }
 #pragma unroll
         for (int t = 0; t < kAb; t++) {
           const int ab = ab0 + t, row = 32 * ab + lane;
@@ -352,7 +331,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const __grid_const
             sts128(offa + (2 * wA) * 128 + 128, expand16(wa >> 16));
           }
         }
-        if constexpr (kPair && !kTmaB) {
+        if constexpr (kPair) {
 #pragma unroll
           for (int r = 0; r < kW / 8; r++) {
             const int w = p_wbase + 8 * r;
@@ -362,7 +341,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const __grid_const
               sts128(offb + (kK / 16) * kSbo, expand32_fp4(ck[r].y));
             }
           }
-        } else if constexpr (!kPair) {
+        } else {
 #pragma unroll
           for (int r = 0; r < kU; r++) {
             const int w = w_base + 4 * r;
@@ -646,34 +625,6 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const __grid_const
   }
 }
 
-// Expanded operand-B rows for the TMA form of the CTA-pair search: out[c][pw][k] = E2M1 bytes
-// of plane c (g_k = c) of SNP k in padded class word pw (class 0's words 0..w0-1 then zero
-// words up to p0, class 1's words from p0, zero words up to p0 + p1), in the same sample order
-// as the threads' expansion.  One thread per (padded word, SNP).
-__global__ void k_expand_b(const uint2* __restrict__ planes, int64_t m_pad, int64_t w0, int64_t w1, int64_t p0,
-                           int64_t p1, uint4* __restrict__ out) {
-  const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t n = (p0 + p1) * m_pad;
-  if (x >= n) return;
-  const int64_t pw = x / m_pad, k = x - pw * m_pad;
-  uint2 v = make_uint2(0, 0);
-  if (pw < p0) {
-    if (pw < w0) v = planes[pw * m_pad + k];
-  } else if (pw - p0 < w1) {
-    v = planes[(w0 + pw - p0) * m_pad + k];
-  }
-  out[x] = expand32_fp4(v.x);
-  out[n + x] = expand32_fp4(v.y);
-}
-
-cudaError_t launch_expand_b(const uint2* planes, int64_t m_pad, int64_t w0, int64_t w1, int64_t p0, int64_t p1,
-                            uint4* out, cudaStream_t stream) {
-  const int64_t n = (p0 + p1) * m_pad;
-  if (n <= 0) return cudaSuccess;
-  k_expand_b<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(planes, m_pad, w0, w1, p0, p1, out);
-  return cudaGetLastError();
-}
-
 // Tile descriptors of one pair-block list: pair block b = (i, j0) holds the tiles
 // [pb_off[b], pb_off[b+1]) with k blocks t = 0, 1, ... (k from j0 + 1 + kK*t); one thread
 // per pair block writes them to out[pb_off[b] ...].
@@ -752,9 +703,9 @@ __global__ void k_fill_slots(BestSlot* __restrict__ slots, int64_t n) {
 
 int tc_warps_per_block() { return kTcWarps; }
 
-template <int kW, bool kF, bool kP, bool kB, bool kD, bool kT, bool kM = false, bool kX = false>
+template <int kW, bool kF, bool kP, bool kB, bool kD, bool kT>
 static cudaError_t set_smem() {
-  return cudaFuncSetAttribute(k_scan_tc<kW, kF, kP, kB, kD, kT, kM, kX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_scan_tc<kW, kF, kP, kB, kD, kT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kTcSmemBytes);
 }
 
@@ -776,10 +727,9 @@ cudaError_t tc_configure() {
     if (e == cudaSuccess) e = set_smem_all<16, true, false>();
     if (e == cudaSuccess) e = set_smem_all<8, true, true>();
     if (e == cudaSuccess) e = set_smem_all<16, true, true>();
-    if (e == cudaSuccess) e = set_smem<16, true, true, false, false, false, true>();  // pair margins
-    if (e == cudaSuccess) e = set_smem<16, true, true, false, false, false, false, true>();  // TMA operand B
-    if (e == cudaSuccess) e = set_smem<16, true, true, false, true, false, false, true>();
-    if (e == cudaSuccess) e = set_smem<16, true, true, false, false, true, false, true>();
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_scan_tc<16, true, true, false, false, false, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
     if (e != cudaSuccess) return e;
     configured = true;
   }
@@ -795,7 +745,7 @@ static void launch_variant(const TcParams& p, int blocks, bool batched, bool dum
 }
 
 // CTA-pair kernels: clusters of two CTAs
-template <int kW, bool kB, bool kD, bool kT, bool kM = false, bool kX = false>
+template <int kW, bool kB, bool kD, bool kT, bool kM = false>
 static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t stream) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)blocks);
@@ -809,7 +759,7 @@ static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t strea
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_scan_tc<kW, true, true, kB, kD, kT, kM, kX>, p);
+  return cudaLaunchKernelEx(&cfg, k_scan_tc<kW, true, true, kB, kD, kT, kM>, p);
 }
 
 template <int kW>
@@ -857,12 +807,7 @@ cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, b
   if (ce != cudaSuccess) return ce;
   const bool topk = p.top_k > 1;
   const bool batched = p.jobs != nullptr;
-  if (fp4 && pair && words_per_stage == 16 && p.use_bexp && !batched) {  // operand B by TMA
-    const cudaError_t e = dump ? launch_pair<16, false, true, false, false, true>(p, blocks & ~1, stream)
-                          : topk ? launch_pair<16, false, false, true, false, true>(p, blocks & ~1, stream)
-                                 : launch_pair<16, false, false, false, false, true>(p, blocks & ~1, stream);
-    if (e != cudaSuccess) return e;
-  } else if (fp4 && pair) {
+  if (fp4 && pair) {
     const cudaError_t e = words_per_stage == 16
                               ? launch_pair_variant<16>(p, blocks & ~1, batched, dump, topk, stream)
                               : launch_pair_variant<8>(p, blocks & ~1, batched, dump, topk, stream);
