@@ -425,7 +425,8 @@ def run_ours(args, rank, world, local_rank):
         # the other forms of the north star, bounded (about 1.5 minutes together), after the
         # timed region: batched, precision and serving
         forms = {}
-        for name, fn in (("precision", precision_form), ("batched", batched_form), ("serving", serving_form)):
+        for name, fn in (("precision", precision_form), ("batched", batched_form), ("replicates", replicates_form),
+                         ("serving", serving_form)):
             t0 = time.perf_counter()
             try:
                 forms[name] = fn()
@@ -573,6 +574,44 @@ def precision_form(steps=3, warmup=1):
                                                               for t, x in zip(top, fx["top"]))}
     except (OSError, KeyError, ValueError):
         out["vs_fp64_oracle"] = None
+    return out
+
+
+def replicates_form(n_a=64, n_b=8):
+    """Permutation replicates of the serving workload's resident matrices (A 1024 SNPs x 8192
+    samples, B 3072 x 4096): the replicate form (all-sample counts shared across replicates,
+    epik2_scan_replicates) against the same replicates searched one by one with the plain
+    kernel (set_pheno + scan each, same CTA-pair FP4 configuration); results must be equal."""
+    import numpy as np
+    import epik2
+    from epik2 import workloads as W
+    out = {}
+    rng = np.random.default_rng(1006)
+    with epik2.Context(0) as ctx:
+        for m, n in zip(W.SERVING["resident"], (n_a, n_b)):
+            g, p = W.generate(m)
+            reps = np.stack([rng.permutation(p) for _ in range(n)])
+            did = ctx.load(g, p)
+            ts = epik2.n_triplets(m["n_snps"]) * m["n_samples"] * n
+            ctx.scan_replicates(did, reps[:2])  # warm-up
+            t0 = time.perf_counter()
+            got = ctx.scan_replicates(did, reps)
+            wall_r = time.perf_counter() - t0
+            kms_r = ctx.stats()["last_scan_kernel_ms"]
+            kms_p, plain = 0.0, []
+            t0 = time.perf_counter()
+            for r in reps:
+                ctx.set_pheno(did, r)
+                plain.append(ctx.scan(did, engine=epik2.ENGINE_TC_FP4, stage_words=16, pair_tile=64, overlap=1))
+                kms_p += ctx.stats()["last_scan_kernel_ms"]
+            wall_p = time.perf_counter() - t0
+            ctx.unload(did)
+            out[m["name"]] = {
+                "replicates": n, "triplet_samples": ts,
+                "replicate_form": {"value": ts / (kms_r / 1e3), "wall_value": ts / wall_r, "kernel_ms": kms_r},
+                "one_by_one_plain": {"value": ts / (kms_p / 1e3), "wall_value": ts / wall_p, "kernel_ms": kms_p},
+                "speedup_kernel": kms_p / kms_r, "speedup_wall": wall_p / wall_r,
+                "results_identical": all(a.ijk == b.ijk and a.score == b.score for a, b in zip(got, plain))}
     return out
 
 

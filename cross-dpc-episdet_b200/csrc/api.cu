@@ -554,17 +554,11 @@ int run_pairs_tc(epik2_ctx* ctx, DevDataset& d) {
   return EPIK2_OK;
 }
 
-// Tensor-core engine: one CTA per SM, tiles = pair blocks (i, j0..j0+31) x k blocks of
-// 128 (int8 format) or 112 (FP4 format) SNPs.
-int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
-                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair,
-                bool overlap) {
-  const int64_t m = d.n_snps;
+// Tile descriptors of the search of first indices [ib, ie) of an m-SNP dataset into
+// ctx->d_tiles (expanded on the GPU from the pair-block list); *n_tiles receives their count.
+int prepare_tiles(epik2_ctx* ctx, int64_t m, int64_t ib, int64_t ie, bool fp4, bool pair, int64_t* n_tiles) {
   const int64_t kk = tc_k_per_tile(fp4);
-  pair = pair && fp4;
-  overlap = overlap && pair;
   const int64_t jstep = pair ? 64 : 32;  // SNPs j per tile (a CTA pair takes 64)
-  const int grid = pair ? tc_pair_blocks(ctx->tc_blocks) : ctx->tc_blocks;
   std::vector<uint32_t> ij;
   std::vector<int64_t> off(1, 0);
   // Pair blocks in the order (u, i) with j0 = i + 1 + jstep*u: consecutive pair blocks (and
@@ -608,6 +602,22 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
        "tile descriptors");
     ctx->stats.kernel_launches += 1;
   }
+  *n_tiles = off.back();
+  return EPIK2_OK;
+}
+
+// Tensor-core engine: one CTA per SM, tiles = pair blocks (i, j0..j0+31) x k blocks of
+// 128 (int8 format) or 112 (FP4 format) SNPs.
+int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
+                float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair,
+                bool overlap) {
+  const int64_t m = d.n_snps;
+  pair = pair && fp4;
+  overlap = overlap && pair;
+  const int grid = pair ? tc_pair_blocks(ctx->tc_blocks) : ctx->tc_blocks;
+  int64_t n_tiles = 0;
+  int r = prepare_tiles(ctx, m, ib, ie, fp4, pair, &n_tiles);
+  if (r) return r;
   CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream), "reset counter");
   CK(ctx, cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream), "reset error word");
   TcParams p{};
@@ -616,7 +626,7 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   p.pairs = d.pairs;
   p.lut = d.lut;
   p.tiles = ctx->d_tiles;
-  p.n_tiles = off.back();
+  p.n_tiles = n_tiles;
   p.tri = d.tri;
   p.m = (int32_t)m;
   p.m_pad = (int32_t)d.m_pad;
@@ -1481,6 +1491,127 @@ int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, cons
                 "(32- or 64-SNP tiles), or 4 or 8 overlapped on 64-SNP tiles");
   const std::vector<int> codes(ds.size(), tc_code(pick.kw, fp4, pick.pair && fp4, pick.overlap));
   return run_batch(ctx, ds, ids, codes, opts && opts->rescore_fp64, out);
+}
+
+int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phenos, int32_t n_reps,
+                          epik2_best* out) {
+  if (!ctx) return EPIK2_E_INVALID;
+  if (!phenos || !out || n_reps < 1) return fail(ctx, EPIK2_E_INVALID, "bad replicate list");
+  DevDataset* base = find(ctx, dataset_id);
+  if (!base) return fail(ctx, EPIK2_E_NOT_FOUND, "unknown dataset");
+  if (base->n_snps < 3) return fail(ctx, EPIK2_E_INVALID, "need at least 3 SNPs");
+  if (!fp4_exact(*base))
+    return fail(ctx, EPIK2_E_TOO_LARGE, "replicate form (FP4 on CTA pairs): a class of 2^24 samples or more");
+  CK(ctx, cudaSetDevice(ctx->device), "set device");
+  const int64_t S = base->n_samples, m = base->n_snps;
+  const int grid = tc_pair_blocks(ctx->tc_blocks);
+  // replicates per launch: as many as fit in free device memory above 1 GiB, at most 256
+  const int64_t rep_bytes = (int64_t)dataset_layout(S, m, false).total;
+  size_t fr = 0, tot = 0;
+  CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
+  const int64_t fit = ((int64_t)fr - ((int64_t)1 << 30)) / std::max<int64_t>(rep_bytes, 1);
+  const int32_t group = (int32_t)std::max<int64_t>(1, std::min<int64_t>({fit, (int64_t)n_reps, 256}));
+  int64_t n_tiles = 0;
+  int r = prepare_tiles(ctx, m, 0, m, true, true, &n_tiles);
+  if (r) return r;
+  TcJob* d_jobs = nullptr;
+  BestSlot *d_rslots = nullptr, *d_res = nullptr;
+  cudaError_t e = cudaMalloc(&d_jobs, sizeof(TcJob) * group);
+  if (e == cudaSuccess) e = cudaMalloc(&d_rslots, sizeof(BestSlot) * (size_t)group * grid);
+  if (e == cudaSuccess) e = cudaMalloc(&d_res, sizeof(BestSlot) * group);
+  std::vector<int32_t> ids;
+  auto release = [&]() {
+    for (int32_t id : ids) epik2_unload(ctx, id);
+    ids.clear();
+    cudaFree(d_jobs);
+    cudaFree(d_rslots);
+    cudaFree(d_res);
+  };
+  if (e != cudaSuccess) {
+    release();
+    return cuda_fail(ctx, e, "replicate buffers");
+  }
+  double kms_total = 0.0;
+  std::vector<TcJob> jobs((size_t)group);
+  std::vector<BestSlot> res((size_t)group);
+  for (int32_t done = 0; done < n_reps; done += group) {
+    const int32_t g = std::min<int32_t>(group, n_reps - done);
+    for (int32_t t = 0; t < g; t++) {  // each replicate's class order, planes, margins
+      int32_t id = -1;
+      r = epik2_load_replicate(ctx, dataset_id, phenos + (size_t)(done + t) * (size_t)S, &id);
+      if (r) {
+        release();
+        return r;
+      }
+      ids.push_back(id);
+      const DevDataset& R = *find(ctx, id);
+      jobs[(size_t)t] = TcJob{R.planes, R.singles, R.pairs, R.lut, R.lut64, R.tri, (int32_t)R.n_snps,
+                              (int32_t)R.m_pad, (int32_t)R.w0, (int32_t)R.w1, (int32_t)R.n_controls,
+                              (int32_t)R.n_cases};
+    }
+    e = cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(TcJob) * g, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_fill_slots(d_rslots, (int64_t)g * grid, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream);
+    TcParams p{};
+    p.planes = base->planes;  // pass 0: all samples of the base dataset
+    p.singles = base->singles;
+    p.pairs = base->pairs;
+    p.lut = base->lut;
+    p.tiles = ctx->d_tiles;
+    p.n_tiles = n_tiles;
+    p.tri = base->tri;
+    p.m = (int32_t)m;
+    p.m_pad = (int32_t)base->m_pad;
+    p.w0 = (int32_t)base->w0;
+    p.w1 = (int32_t)base->w1;
+    p.n0 = (int32_t)base->n_controls;
+    p.n1 = (int32_t)base->n_cases;
+    p.counter = ctx->d_counter;
+    p.slots = ctx->d_slots;
+    p.err = ctx->d_err;
+    p.wait_limit = ctx->wait_limit;
+    p.jobs = d_jobs;
+    p.n_jobs = g;
+    p.n_reps = g;
+    p.job_slots = d_rslots;
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_start, ctx->stream);
+    if (e == cudaSuccess) e = launch_scan_reps(p, grid, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_stop, ctx->stream);
+    if (e == cudaSuccess) e = launch_reduce_jobs(d_rslots, g, grid, d_res, ctx->stream);
+    int err_word = 0;
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(res.data(), d_res, sizeof(BestSlot) * g, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&err_word, ctx->d_err, 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    float kms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&kms, ctx->ev_start, ctx->ev_stop);
+    if (e != cudaSuccess) {
+      release();
+      return cuda_fail(ctx, e, "replicate search");
+    }
+    if (err_word) {
+      release();
+      return fail(ctx, EPIK2_E_TIMEOUT, "replicate search: a bounded wait expired");
+    }
+    ctx->stats.kernel_launches += 3;
+    ctx->stats.h2d_bytes += sizeof(TcJob) * g;
+    ctx->stats.d2h_bytes += sizeof(BestSlot) * g + 4;
+    kms_total += kms;
+    for (int32_t t = 0; t < g; t++) {
+      epik2_best& b = out[done + t];
+      b.score = res[(size_t)t].score;
+      b.score_fp64 = std::numeric_limits<double>::quiet_NaN();
+      decode_key(res[(size_t)t].key, b.i, b.j, b.k);
+    }
+    for (int32_t id : ids) epik2_unload(ctx, id);
+    ids.clear();
+  }
+  release();
+  ctx->stats.last_scan_kernel_ms = kms_total;
+  ctx->stats.last_scan_triplets = triplets_before(m, m) * n_reps;
+  ctx->stats.last_scan_words = 0;
+  return EPIK2_OK;
 }
 
 int epik2_dump_tables(epik2_ctx* ctx, int32_t dataset_id, uint32_t* tables, float* scores) {

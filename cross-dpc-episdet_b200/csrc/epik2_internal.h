@@ -138,6 +138,9 @@ struct TcParams {
   long long wait_limit;
   // test hook: CTA 0 withholds one arrival so that its first wait expires (single CTAs)
   int32_t test_withhold;
+  // replicate form (launch_scan_reps): jobs = the n_reps replicates of the base dataset
+  // (p.planes ... p.n1), job_slots = [n_reps][grid] per-replicate results
+  int32_t n_reps;
 };
 
 // Kernel launchers (scan_int.cu / scan_tc.cu / encode.cu); all asynchronous on `stream`.
@@ -145,6 +148,8 @@ cudaError_t launch_encode(const DevDataset& d, cudaStream_t stream);
 cudaError_t launch_counts(const DevDataset& d, cudaStream_t stream, bool pairs = true);
 // pair margins on tensor cores (the CTA-pair FP4 kernel; exact for classes below 2^24)
 cudaError_t launch_pairs_tc(const TcParams& p, int blocks, cudaStream_t stream);
+// replicate form of the CTA-pair FP4 search (16 words per stage): see TcParams::n_reps
+cudaError_t launch_scan_reps(const TcParams& p, int blocks, cudaStream_t stream);
 cudaError_t launch_scan_int(const ScanParams& p, int blocks, bool dump, cudaStream_t stream);
 cudaError_t launch_reduce_best(const BestSlot* slots, int n, BestSlot* out, cudaStream_t stream);
 cudaError_t launch_tables(const DevDataset& d, const uint32_t* triplets, int64_t n, uint32_t* out,

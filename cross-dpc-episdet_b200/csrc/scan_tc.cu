@@ -78,10 +78,18 @@ struct JobView {
 // kMarg (CTA pairs only): the pair-margin form.  Operand A's g_i = 0 rows are all ones and
 // its g_i = 1 rows zero, so D[(j, 0, b)][(k, c)] is the count of (g_j = b, g_k = c): tiles
 // (0, j0, k block) write the pair margins of every j < k < m_pad instead of scoring.
-template <int kW, bool kFp4, bool kPair, bool kBatched, bool kDump, bool kTopK, bool kMarg = false>
+// kRepl (CTA pairs, 16 words per stage): the replicate form.  The tile's passes share one
+// pair operand expansion scheme and the tensor memory: pass 0 counts all samples of the base
+// dataset (its two classes' words as one range) into the class-0 accumulators, where they stay;
+// pass r = 1..p.n_reps counts the cases of replicate r (p.jobs[r-1]) into the class-1
+// accumulators and scores replicate r with controls = totals - cases, its best folded into
+// p.job_slots[r-1].  Permutation replicates of one matrix thus share the all-sample counts.
+template <int kW, bool kFp4, bool kPair, bool kBatched, bool kDump, bool kTopK, bool kMarg = false,
+          bool kRepl = false>
 __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) {
   static_assert(!kPair || kFp4, "CTA pairs use the FP4 format");
   static_assert(!kMarg || (kPair && !kBatched && !kDump && !kTopK), "pair margins: plain CTA-pair kernel");
+  static_assert(!kRepl || (kPair && kW == 16 && !kBatched && !kDump && !kTopK && !kMarg), "replicates: CTA pairs");
   constexpr int kK = kFp4 ? 112 : 128;                // SNPs k per tile -> 2*kK rows of B
   constexpr int kRowBytes = (kFp4 ? 16 : 32) * kW;    // operand bytes per row per stage
   constexpr int kBRows = kPair ? kK : 2 * kK;         // B rows held by this CTA
@@ -249,9 +257,18 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     } else {
       jv = JobView{p.planes, p.singles, p.pairs, p.lut, p.tri, p.m, p.m_pad, p.w0, p.w1, p.n0, p.n1};
     }
+    const int n_pass = kRepl ? 1 + p.n_reps : 1;
+    for (int pass = 0; pass < n_pass; pass++) {
+    if (kRepl && pass > 0) {  // replicate `pass`: its planes, class split, margins and table
+      const TcJob& R = p.jobs[pass - 1];
+      jv = JobView{R.planes, R.singles, R.pairs, R.lut, R.tri, R.m, R.m_pad, R.w0, R.w1, R.n0, R.n1};
+    }
     const int64_t m_pad = jv.m_pad;
     const int m = jv.m;
-    const int nc0 = (jv.w0 + kW - 1) / kW, nc1 = (jv.w1 + kW - 1) / kW, nct = nc0 + nc1;
+    // words counted into class 0 and class 1 in this pass (class-1 words start at jv.w0)
+    const int lim0 = kRepl ? (pass == 0 ? jv.w0 + jv.w1 : 0) : jv.w0;
+    const int lim1 = kRepl ? (pass == 0 ? 0 : jv.w1) : jv.w1;
+    const int nc0 = (lim0 + kW - 1) / kW, nc1 = (lim1 + kW - 1) / kW, nct = nc0 + nc1;
 
     // ---- operand expansion and MMA, 32*kW samples per stage ----
     // Work of a stage per thread:
@@ -278,7 +295,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     auto load_words = [&](int cc, uint2& gi, uint2& gj, uint2 (&gk)[kUB]) {
       const bool c1 = cc >= nc0;
       const int c_in = c1 ? cc - nc0 : cc;
-      const int wcls = c1 ? jv.w1 : jv.w0;
+      const int wcls = c1 ? lim1 : lim0;
       const int64_t wb = (c1 ? (int64_t)jv.w0 : 0) + (int64_t)kW * c_in;
       gi = make_uint2(0, 0);
       gj = gi;
@@ -408,7 +425,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         }
         if (kPair) {
           mma_commit_pair(bar0 + 8 * s);
-          if (cc == nct - 1) mma_commit_pair(bar_acc);
+          if (cc == nct - 1 && !(kRepl && pass == 0)) mma_commit_pair(bar_acc);  // pass 0 is not scored
         } else {
           mma_commit(bar0 + 8 * s);
           if (cc == nct - 1) mma_commit(bar_acc);
@@ -419,6 +436,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     __syncwarp();
     __syncthreads();  // every thread has left the stage loop (done, or an expired wait)
     if (*abort_flag) break;
+    if (kRepl && pass == 0) continue;  // the totals stay in tensor memory for the replicates
 
     // ---- epilogue: TMEM -> shared -> complete tables, score, select ----
     {
@@ -453,7 +471,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         // go to E[cls][lane][56c + kp], 7 groups of 16 columns per class and lane quarter
 #pragma unroll
         for (int cls = 0; cls < 2; cls++) {
-          const bool has = (cls ? nc1 > 0 : nc0 > 0) && worker;
+          const bool has = (cls ? nc1 > 0 : (kRepl || nc0 > 0)) && worker;
 #pragma unroll
           for (int t = 0; t < 2; t++) {
             const int u = cgrp + 4 * t;  // warp-uniform
@@ -544,6 +562,10 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
               t80[2 * ab + c] = E[(0 * 128 + 32 * ab + q) * kEStride + kEc * c + kl];
               t81[2 * ab + c] = E[(1 * 128 + 32 * ab + q) * kEStride + kEc * c + kl];
             }
+          if (kRepl) {  // class 0 holds all samples: the replicate's controls are the rest
+#pragma unroll
+            for (int x = 0; x < 8; x++) t80[x] -= t81[x];
+          }
           const uint2 sj0 = *reinterpret_cast<const uint2*>(jv.singles + ((int64_t)j) * 2);
           const uint2 sj1 = *reinterpret_cast<const uint2*>(jv.singles + (m_pad + j) * 2);
           const uint2 sk0 = *reinterpret_cast<const uint2*>(jv.singles + ((int64_t)k) * 2);
@@ -589,6 +611,9 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
       }
       __syncthreads();  // the staging buffer is rewritten by the next half / next tile
     }
+    if (kRepl) flush_job(pass - 1);  // replicate `pass`'s best of this tile into its slot
+    }  // passes
+    if (*abort_flag) break;
   }
 
   // ---- teardown: every MMA has completed (its tile's accumulator barrier was waited) ----
@@ -603,7 +628,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     else
       asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
   }
-  if (!kBatched && worker) {
+  if (!kBatched && !kRepl && worker) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       const float os = __shfl_xor_sync(kFull, best_s, off);
@@ -703,9 +728,9 @@ __global__ void k_fill_slots(BestSlot* __restrict__ slots, int64_t n) {
 
 int tc_warps_per_block() { return kTcWarps; }
 
-template <int kW, bool kF, bool kP, bool kB, bool kD, bool kT>
+template <int kW, bool kF, bool kP, bool kB, bool kD, bool kT, bool kM = false, bool kR = false>
 static cudaError_t set_smem() {
-  return cudaFuncSetAttribute(k_scan_tc<kW, kF, kP, kB, kD, kT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_scan_tc<kW, kF, kP, kB, kD, kT, kM, kR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kTcSmemBytes);
 }
 
@@ -727,9 +752,8 @@ cudaError_t tc_configure() {
     if (e == cudaSuccess) e = set_smem_all<16, true, false>();
     if (e == cudaSuccess) e = set_smem_all<8, true, true>();
     if (e == cudaSuccess) e = set_smem_all<16, true, true>();
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_scan_tc<16, true, true, false, false, false, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
+    if (e == cudaSuccess) e = set_smem<16, true, true, false, false, false, true>();         // pair margins
+    if (e == cudaSuccess) e = set_smem<16, true, true, false, false, false, false, true>();  // replicates
     if (e != cudaSuccess) return e;
     configured = true;
   }
@@ -745,7 +769,7 @@ static void launch_variant(const TcParams& p, int blocks, bool batched, bool dum
 }
 
 // CTA-pair kernels: clusters of two CTAs
-template <int kW, bool kB, bool kD, bool kT, bool kM = false>
+template <int kW, bool kB, bool kD, bool kT, bool kM = false, bool kR = false>
 static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t stream) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)blocks);
@@ -759,7 +783,7 @@ static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t strea
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_scan_tc<kW, true, true, kB, kD, kT, kM>, p);
+  return cudaLaunchKernelEx(&cfg, k_scan_tc<kW, true, true, kB, kD, kT, kM, kR>, p);
 }
 
 template <int kW>
@@ -820,6 +844,13 @@ cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, b
     else launch_variant<4, false>(p, blocks, batched, dump, topk, stream);
   }
   return cudaGetLastError();
+}
+
+cudaError_t launch_scan_reps(const TcParams& p, int blocks, cudaStream_t stream) {
+  const cudaError_t ce = tc_configure();
+  if (ce != cudaSuccess) return ce;
+  const cudaError_t e = launch_pair<16, false, false, false, false, true>(p, blocks & ~1, stream);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_pairs_tc(const TcParams& p, int blocks, cudaStream_t stream) {

@@ -236,6 +236,17 @@ int epik2_scan_u8(epik2_ctx *ctx, const uint8_t *geno, const uint8_t *pheno, int
 int epik2_scan_batch(epik2_ctx *ctx, const int32_t *dataset_ids, int32_t n, const epik2_opts *opts,
                      epik2_best *out);
 
+/* Replicate form (no reference counterpart; the phenotype-mask idea of GPU/v1.cpp:264-289 on
+ * tensor cores): the best triplet of each of n_reps phenotype-permutation replicates of a
+ * resident dataset (phenos: n_reps x n_samples bytes, 1 = case).  Each tile of the search
+ * counts the all-sample contingency cells of the base matrix once, then for every replicate
+ * only its cases; its controls are the totals minus its cases.  Runs the FP4 CTA-pair kernel
+ * (EPIK2_E_TOO_LARGE for classes of 2^24 samples or more), as many replicates per launch as
+ * free device memory allows (at most 256).  out[r] equals epik2_scan of the dataset with
+ * phenotype r. */
+int epik2_scan_replicates(epik2_ctx *ctx, int32_t dataset_id, const uint8_t *phenos, int32_t n_reps,
+                          epik2_best *out);
+
 /* Autotuner (no reference counterpart).  Times nine configurations on a slice of the
  * dataset (about 1/64 of its triplets, at least a few tiles per SM): the integer engine; the
  * int8 tensor-core engine at 4 and 8 words (128 and 256 samples) per stage; and, when its

@@ -1,0 +1,70 @@
+"""Replicate form: permutation replicates of one resident matrix searched with shared
+all-sample counts (GPU).
+
+Every tile counts the base matrix's all-sample cells once and then, per replicate, only the
+replicate's cases; controls are the totals minus the cases.  Each replicate's best triplet and
+FP32 score must equal a plain search of the matrix with that phenotype (and the oracle's), bit
+for bit, including replicates with no cases or no controls, ragged sample and SNP counts, and
+more replicates than one launch takes (256)."""
+import numpy as np
+import pytest
+
+import epik2
+import oracle as O
+from conftest import f32_bits
+
+pytestmark = pytest.mark.gpu
+
+
+def _perms(p, n, seed):
+    rng = np.random.default_rng(seed)
+    return np.stack([rng.permutation(p) for _ in range(n)])
+
+
+@pytest.mark.parametrize("seed,S,M,cases,R", [(131, 1000, 150, 400, 1), (132, 777, 97, 300, 7), (133, 2049, 70, 1500, 32)])
+def test_replicates_equal_plain_searches_and_oracle(seed, S, M, cases, R):
+    g, p = O.gen_hwe(seed, S, M, cases, planted=[(3, 40, M - 5)], effects=[0.8])
+    reps = _perms(p, R, seed)
+    with epik2.Context(0) as ctx:
+        base = ctx.load(g, p)
+        got = ctx.scan_replicates(base, reps)
+        plain = []
+        for r in reps:
+            ctx.set_pheno(base, r)
+            plain.append(ctx.scan(base, engine=epik2.ENGINE_TC_FP4, stage_words=16, pair_tile=64, overlap=1))
+        ctx.unload(base)
+    assert len(got) == R
+    for a, b in zip(got, plain):
+        assert a.ijk == b.ijk and f32_bits(a.score) == f32_bits(b.score)
+    for r, a in list(zip(reps, got))[:3]:
+        ref = O.scan(g, r)
+        assert a.ijk == ref["ijk"] and f32_bits(a.score) == f32_bits(ref["score"])
+
+
+def test_replicates_without_cases_or_controls():
+    """A replicate whose phenotype has no cases (its cases' accumulators are never written in
+    that pass) or only cases (no controls) still gets the oracle's result."""
+    g, p = O.gen_hwe(134, 600, 40, 300)
+    reps = np.stack([np.zeros(600, np.uint8), np.ones(600, np.uint8), p, np.roll(p, 7)])
+    with epik2.Context(0) as ctx:
+        base = ctx.load(g, p)
+        got = ctx.scan_replicates(base, reps)
+        ctx.unload(base)
+    for r, a in zip(reps, got):
+        ref = O.scan(g, r)
+        assert a.ijk == ref["ijk"] and f32_bits(a.score) == f32_bits(ref["score"])
+
+
+def test_more_replicates_than_one_launch():
+    g, p = O.gen_hwe(135, 200, 20, 90)
+    reps = _perms(p, 300, 135)
+    with epik2.Context(0) as ctx:
+        base = ctx.load(g, p)
+        got = ctx.scan_replicates(base, reps)
+        plain = []
+        for r in reps:
+            ctx.set_pheno(base, r)
+            plain.append(ctx.scan(base, engine=epik2.ENGINE_TC_FP4, stage_words=16, pair_tile=64, overlap=1))
+        ctx.unload(base)
+    assert [a.ijk for a in got] == [b.ijk for b in plain]
+    assert [f32_bits(a.score) for a in got] == [f32_bits(b.score) for b in plain]
