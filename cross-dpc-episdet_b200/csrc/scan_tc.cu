@@ -431,6 +431,9 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
           if (cc == nct - 1) mma_commit(bar_acc);
         }
       }
+      // a replicate without cases has no products of its own: the accumulator barrier still
+      // completes, once the totals of pass 0 are in
+      if (kRepl && pass > 0 && nct == 0 && !*abort_flag) mma_commit_pair(bar_acc);
     }
     g_chunk += (uint32_t)nct;
     __syncwarp();
