@@ -1494,7 +1494,7 @@ int epik2_scan_batch(epik2_ctx* ctx, const int32_t* dataset_ids, int32_t n, cons
 }
 
 int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phenos, int32_t n_reps,
-                          epik2_best* out) {
+                          const epik2_opts* opts, epik2_best* out) {
   if (!ctx) return EPIK2_E_INVALID;
   if (!phenos || !out || n_reps < 1) return fail(ctx, EPIK2_E_INVALID, "bad replicate list");
   DevDataset* base = find(ctx, dataset_id);
@@ -1511,14 +1511,15 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
   const int64_t fit = ((int64_t)fr - ((int64_t)1 << 30)) / std::max<int64_t>(rep_bytes, 1);
   const int32_t group = (int32_t)std::max<int64_t>(1, std::min<int64_t>({fit, (int64_t)n_reps, 256}));
-  int64_t n_tiles = 0;
-  int r = prepare_tiles(ctx, m, 0, m, true, true, &n_tiles);
-  if (r) return r;
+  int r = EPIK2_OK;
+  const bool rescore = opts && opts->rescore_fp64;
   TcJob* d_jobs = nullptr;
   BestSlot *d_rslots = nullptr, *d_res = nullptr;
+  Rescored* d_resc = nullptr;
   cudaError_t e = cudaMalloc(&d_jobs, sizeof(TcJob) * group);
   if (e == cudaSuccess) e = cudaMalloc(&d_rslots, sizeof(BestSlot) * (size_t)group * grid);
   if (e == cudaSuccess) e = cudaMalloc(&d_res, sizeof(BestSlot) * group);
+  if (e == cudaSuccess) e = cudaMalloc(&d_resc, sizeof(Rescored) * group);
   std::vector<int32_t> ids;
   auto release = [&]() {
     for (int32_t id : ids) epik2_unload(ctx, id);
@@ -1526,6 +1527,7 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
     cudaFree(d_jobs);
     cudaFree(d_rslots);
     cudaFree(d_res);
+    cudaFree(d_resc);
   };
   if (e != cudaSuccess) {
     release();
@@ -1534,6 +1536,7 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   double kms_total = 0.0;
   std::vector<TcJob> jobs((size_t)group);
   std::vector<BestSlot> res((size_t)group);
+  std::vector<Rescored> resc((size_t)group);
   for (int32_t done = 0; done < n_reps; done += group) {
     const int32_t g = std::min<int32_t>(group, n_reps - done);
     for (int32_t t = 0; t < g; t++) {  // each replicate's class order, planes, margins
@@ -1548,6 +1551,14 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
       jobs[(size_t)t] = TcJob{R.planes, R.singles, R.pairs, R.lut, R.lut64, R.tri, (int32_t)R.n_snps,
                               (int32_t)R.m_pad, (int32_t)R.w0, (int32_t)R.w1, (int32_t)R.n_controls,
                               (int32_t)R.n_cases};
+    }
+    // the search's tile descriptors, after the replicates' loads (their pair margins use the
+    // same descriptor buffer)
+    int64_t n_tiles = 0;
+    r = prepare_tiles(ctx, m, 0, m, true, true, &n_tiles);
+    if (r) {
+      release();
+      return r;
     }
     e = cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(TcJob) * g, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = launch_fill_slots(d_rslots, (int64_t)g * grid, ctx->stream);
@@ -1579,6 +1590,9 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
     if (e == cudaSuccess) e = launch_scan_reps(p, grid, ctx->stream);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_stop, ctx->stream);
     if (e == cudaSuccess) e = launch_reduce_jobs(d_rslots, g, grid, d_res, ctx->stream);
+    if (e == cudaSuccess && rescore) e = launch_rescore_jobs(d_jobs, d_res, g, d_resc, ctx->stream);
+    if (e == cudaSuccess && rescore)
+      e = cudaMemcpyAsync(resc.data(), d_resc, sizeof(Rescored) * g, cudaMemcpyDeviceToHost, ctx->stream);
     int err_word = 0;
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(res.data(), d_res, sizeof(BestSlot) * g, cudaMemcpyDeviceToHost, ctx->stream);
@@ -1601,7 +1615,7 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
     for (int32_t t = 0; t < g; t++) {
       epik2_best& b = out[done + t];
       b.score = res[(size_t)t].score;
-      b.score_fp64 = std::numeric_limits<double>::quiet_NaN();
+      b.score_fp64 = rescore ? resc[(size_t)t].s64 : std::numeric_limits<double>::quiet_NaN();
       decode_key(res[(size_t)t].key, b.i, b.j, b.k);
     }
     for (int32_t id : ids) epik2_unload(ctx, id);

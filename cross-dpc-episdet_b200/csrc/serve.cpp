@@ -6,8 +6,10 @@
 // turn (round robin from where the previous round stopped, so a small request is not held
 // behind a large one); create each admitted scan's dataset (a replicate sharing a
 // resident genotype matrix, or a freshly uploaded matrix); run one batched launch over
-// all of them (epik2_scan_batch); release the datasets; and complete the requests whose
-// scans are all done.  Requests that arrive during a launch join the next admission
+// all of them (epik2_scan_batch) -- except that two or more replicates of one resident matrix
+// admitted together run in the replicate form (epik2_scan_replicates: each tile's all-sample
+// counts shared by them); release the datasets; and complete the requests whose scans are
+// all done.  Requests that arrive during a launch join the next admission
 // round.  Submitting never waits for the device: it copies the request and queues it.
 #include <algorithm>
 #include <atomic>
@@ -159,11 +161,37 @@ struct epik2_server {
       std::vector<size_t> ok_items;
       std::vector<int> status(batch.size(), EPIK2_OK);
       std::vector<epik2_best> res;
+      std::vector<epik2_best> rep_res(batch.size());
+      std::vector<char> in_rep(batch.size(), 0);  // scanned in the replicate form
       for (int spin = 0; spin < 1000 && ctx_waiters.load() > 0; spin++)  // let add_matrix in first
         std::this_thread::sleep_for(std::chrono::microseconds(100));
       {
         std::lock_guard<std::mutex> g(ctx_mu);
+        // replicate scans of one resident matrix (two or more in this launch) run in the
+        // replicate form: each tile's all-sample counts are shared by the replicates
+        std::map<int32_t, std::vector<size_t>> by_matrix;
+        for (size_t b = 0; b < batch.size(); b++)
+          if (batch[b].req->dataset >= 0) by_matrix[batch[b].req->dataset].push_back(b);
+        for (auto& kv : by_matrix) {
+          if (kv.second.size() < 2 || batch[kv.second[0]].req->n_samples >= (1 << 24)) continue;
+          const size_t s_n = (size_t)batch[kv.second[0]].req->n_samples;
+          std::vector<uint8_t> ph(kv.second.size() * s_n);
+          for (size_t t = 0; t < kv.second.size(); t++) {
+            const Item& it = batch[kv.second[t]];
+            std::memcpy(ph.data() + t * s_n, it.req->phenos.data() + (size_t)it.scan * s_n, s_n);
+          }
+          std::vector<epik2_best> out(kv.second.size());
+          epik2_opts o{};
+          o.rescore_fp64 = opts.rescore_fp64;
+          const int st = epik2_scan_replicates(ctx, kv.first, ph.data(), (int32_t)kv.second.size(), &o, out.data());
+          for (size_t t = 0; t < kv.second.size(); t++) {
+            status[kv.second[t]] = st;
+            rep_res[kv.second[t]] = out[t];
+            in_rep[kv.second[t]] = 1;
+          }
+        }
         for (size_t b = 0; b < batch.size(); b++) {
+          if (in_rep[b]) continue;
           Request* r = batch[b].req;
           const uint8_t* ph = r->phenos.data() + (size_t)batch[b].scan * (size_t)r->n_samples;
           int32_t id = -1;
@@ -195,6 +223,7 @@ struct epik2_server {
         for (size_t b = 0; b < batch.size(); b++) {
           Request* r = batch[b].req;
           const epik2_best* rb = nullptr;
+          if (in_rep[b] && status[b] == EPIK2_OK) rb = &rep_res[b];
           if (q < ok_items.size() && ok_items[q] == b) {
             if (status[b] == EPIK2_OK) rb = &res[q];
             q++;

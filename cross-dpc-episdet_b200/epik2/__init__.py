@@ -158,7 +158,7 @@ def library():
         "epik2_read_plink": ([ctypes.c_char_p, ctypes.c_uint8, p, p], ctypes.c_int),
         "epik2_perm_pvalue": ([ctypes.c_float, p, ctypes.c_int64], ctypes.c_double),
         "epik2_scan_batch": ([p, p, i32, ctypes.POINTER(Opts), ctypes.POINTER(Best)], ctypes.c_int),
-        "epik2_scan_replicates": ([p, i32, p, i32, ctypes.POINTER(Best)], ctypes.c_int),
+        "epik2_scan_replicates": ([p, i32, p, i32, ctypes.POINTER(Opts), ctypes.POINTER(Best)], ctypes.c_int),
         "epik2_autotune": ([p, i32, ctypes.POINTER(Tune)], ctypes.c_int),
         "epik2_load_replicate": ([p, i32, p, ctypes.POINTER(i32)], ctypes.c_int),
         "epik2_replicate_bytes": ([i64, i64], i64),
@@ -424,12 +424,14 @@ class Context:
         self._check(self._lib.epik2_scan_batch(self._h, _ptr(ids), len(ids), ctypes.byref(o), arr))
         return [arr[t] for t in range(len(ids))]
 
-    def scan_replicates(self, dataset, phenos):
+    def scan_replicates(self, dataset, phenos, **opts):
         """Best triplet of each phenotype-permutation replicate (rows of phenos) of a resident
         dataset, the all-sample counts shared across replicates (epik2_scan_replicates)."""
         phenos = np.ascontiguousarray(np.atleast_2d(phenos), dtype=np.uint8)
         arr = (Best * len(phenos))()
-        self._check(self._lib.epik2_scan_replicates(self._h, dataset, _ptr(phenos), len(phenos), arr))
+        o = self._opts(**opts)
+        self._check(self._lib.epik2_scan_replicates(self._h, dataset, _ptr(phenos), len(phenos), ctypes.byref(o),
+                                                    arr))
         return [arr[t] for t in range(len(phenos))]
 
     def autotune(self, dataset):

@@ -243,9 +243,10 @@ int epik2_scan_batch(epik2_ctx *ctx, const int32_t *dataset_ids, int32_t n, cons
  * only its cases; its controls are the totals minus its cases.  Runs the FP4 CTA-pair kernel
  * (EPIK2_E_TOO_LARGE for classes of 2^24 samples or more), as many replicates per launch as
  * free device memory allows (at most 256).  out[r] equals epik2_scan of the dataset with
- * phenotype r. */
+ * phenotype r; with opts->rescore_fp64, out[r].score_fp64 is its best triplet rescored in FP64
+ * on the GPU (other options are ignored). */
 int epik2_scan_replicates(epik2_ctx *ctx, int32_t dataset_id, const uint8_t *phenos, int32_t n_reps,
-                          epik2_best *out);
+                          const epik2_opts *opts, epik2_best *out);
 
 /* Autotuner (no reference counterpart).  Times nine configurations on a slice of the
  * dataset (about 1/64 of its triplets, at least a few tiles per SM): the integer engine; the

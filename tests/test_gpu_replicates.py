@@ -68,3 +68,23 @@ def test_more_replicates_than_one_launch():
         ctx.unload(base)
     assert [a.ijk for a in got] == [b.ijk for b in plain]
     assert [f32_bits(a.score) for a in got] == [f32_bits(b.score) for b in plain]
+
+
+def test_early_tiles_of_the_queue_are_searched():
+    """The replicates' own loads compute pair margins with the tensor-core kernel, which uses a
+    descriptor buffer of its own kind: the search's tiles must be laid down after them.  A
+    triplet planted in the first tiles of the queue (first index 2, SNPs 5 and 40) on a 700-SNP
+    matrix is the best of the unpermuted replicate, as a plain search finds."""
+    g, p = O.gen_hwe(136, 1000, 700, 500, maf=(0.3, 0.5), planted=[(2, 5, 40)], effects=[0.9])
+    reps = np.concatenate([p[None, :], _perms(p, 3, 136)])
+    with epik2.Context(0) as ctx:
+        base = ctx.load(g, p)
+        got = ctx.scan_replicates(base, reps)
+        plain = []
+        for r in reps:
+            ctx.set_pheno(base, r)
+            plain.append(ctx.scan(base, engine=epik2.ENGINE_TC_FP4, stage_words=16, pair_tile=64, overlap=1))
+        ctx.unload(base)
+    assert got[0].ijk == (2, 5, 40)
+    for a, b in zip(got, plain):
+        assert a.ijk == b.ijk and f32_bits(a.score) == f32_bits(b.score)
