@@ -1505,25 +1505,30 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   CK(ctx, cudaSetDevice(ctx->device), "set device");
   const int64_t S = base->n_samples, m = base->n_snps;
   const int grid = tc_pair_blocks(ctx->tc_blocks);
-  // replicates per launch: as many as fit in free device memory above 1 GiB, at most 256
-  const int64_t rep_bytes = (int64_t)dataset_layout(S, m, false).total;
+  // replicates per launch: as many as fit in free device memory above 1 GiB, at most 256.
+  // Their class orders, planes and margins live in one allocation for the whole call (one
+  // allocation and one release instead of one per replicate); their genotypes and ln n!
+  // tables are the base dataset's.
+  const Layout L = dataset_layout(S, m, false);
+  const size_t rep_bytes = align_up(L.total, 256);
   size_t fr = 0, tot = 0;
   CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
-  const int64_t fit = ((int64_t)fr - ((int64_t)1 << 30)) / std::max<int64_t>(rep_bytes, 1);
+  const int64_t fit = ((int64_t)fr - ((int64_t)1 << 30)) / (int64_t)rep_bytes;
   const int32_t group = (int32_t)std::max<int64_t>(1, std::min<int64_t>({fit, (int64_t)n_reps, 256}));
   int r = EPIK2_OK;
   const bool rescore = opts && opts->rescore_fp64;
   TcJob* d_jobs = nullptr;
   BestSlot *d_rslots = nullptr, *d_res = nullptr;
   Rescored* d_resc = nullptr;
+  char* arena = nullptr;
   cudaError_t e = cudaMalloc(&d_jobs, sizeof(TcJob) * group);
   if (e == cudaSuccess) e = cudaMalloc(&d_rslots, sizeof(BestSlot) * (size_t)group * grid);
   if (e == cudaSuccess) e = cudaMalloc(&d_res, sizeof(BestSlot) * group);
   if (e == cudaSuccess) e = cudaMalloc(&d_resc, sizeof(Rescored) * group);
-  std::vector<int32_t> ids;
+  if (e == cudaSuccess) e = cudaMalloc(&arena, rep_bytes * (size_t)group);
   auto release = [&]() {
-    for (int32_t id : ids) epik2_unload(ctx, id);
-    ids.clear();
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(arena);
     cudaFree(d_jobs);
     cudaFree(d_rslots);
     cudaFree(d_res);
@@ -1531,23 +1536,40 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   };
   if (e != cudaSuccess) {
     release();
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      return fail(ctx, EPIK2_E_NOMEM, "replicate buffers do not fit in free device memory");
+    }
     return cuda_fail(ctx, e, "replicate buffers");
   }
   double kms_total = 0.0;
   std::vector<TcJob> jobs((size_t)group);
   std::vector<BestSlot> res((size_t)group);
   std::vector<Rescored> resc((size_t)group);
+  std::vector<DevDataset> reps((size_t)group);
   for (int32_t done = 0; done < n_reps; done += group) {
     const int32_t g = std::min<int32_t>(group, n_reps - done);
     for (int32_t t = 0; t < g; t++) {  // each replicate's class order, planes, margins
-      int32_t id = -1;
-      r = epik2_load_replicate(ctx, dataset_id, phenos + (size_t)(done + t) * (size_t)S, &id);
+      DevDataset& R = reps[(size_t)t];
+      char* b = arena + rep_bytes * (size_t)t;
+      R = DevDataset{};
+      R.n_samples = S;
+      R.n_snps = m;
+      R.m_pad = base->m_pad;
+      R.tri = base->tri;
+      R.geno = base->geno;
+      R.lut = base->lut;
+      R.lut64 = base->lut64;
+      R.perm = (int32_t*)(b + L.perm);
+      R.planes = (uint2*)(b + L.planes);
+      R.singles = (uint32_t*)(b + L.singles);
+      R.pairs = (uint4*)(b + L.pairs);
+      R.bytes = L.total;
+      r = encode_with(ctx, R, phenos + (size_t)(done + t) * (size_t)S);
       if (r) {
         release();
         return r;
       }
-      ids.push_back(id);
-      const DevDataset& R = *find(ctx, id);
       jobs[(size_t)t] = TcJob{R.planes, R.singles, R.pairs, R.lut, R.lut64, R.tri, (int32_t)R.n_snps,
                               (int32_t)R.m_pad, (int32_t)R.w0, (int32_t)R.w1, (int32_t)R.n_controls,
                               (int32_t)R.n_cases};
@@ -1618,8 +1640,6 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
       b.score_fp64 = rescore ? resc[(size_t)t].s64 : std::numeric_limits<double>::quiet_NaN();
       decode_key(res[(size_t)t].key, b.i, b.j, b.k);
     }
-    for (int32_t id : ids) epik2_unload(ctx, id);
-    ids.clear();
   }
   release();
   ctx->stats.last_scan_kernel_ms = kms_total;
