@@ -1068,7 +1068,9 @@ int epik2_device_name(const epik2_ctx* ctx, char* buf, size_t len) {
 int epik2_mem_info(const epik2_ctx* ctx, size_t* free_bytes, size_t* total_bytes) {
   if (!ctx || !free_bytes || !total_bytes) return EPIK2_E_INVALID;
   cudaSetDevice(ctx->device);
-  return cudaMemGetInfo(free_bytes, total_bytes) == cudaSuccess ? EPIK2_OK : EPIK2_E_CUDA;
+  if (cudaMemGetInfo(free_bytes, total_bytes) != cudaSuccess) return EPIK2_E_CUDA;
+  *free_bytes += ctx->spare_bytes;  // the context's spare allocation is reused or released on demand
+  return EPIK2_OK;
 }
 
 int epik2_set_stream(epik2_ctx* ctx, void* cuda_stream) {
@@ -1262,7 +1264,8 @@ int epik2_load_replicate(epik2_ctx* ctx, int32_t base_dataset_id, const uint8_t*
   const Layout L = dataset_layout(root->n_samples, root->n_snps, false);
   size_t fr = 0, tot = 0;
   CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
-  if (L.total + (size_t)(256u << 20) > fr) return fail(ctx, EPIK2_E_NOMEM, "replicate does not fit in free device memory");
+  if (L.total + (size_t)(256u << 20) > fr + ctx->spare_bytes)
+    return fail(ctx, EPIK2_E_NOMEM, "replicate does not fit in free device memory");
   std::unique_ptr<DevDataset> d(new DevDataset());
   CK(ctx, take_block(ctx, L.total, &d->block, &d->block_bytes), "alloc replicate");
   char* b = (char*)d->block;
@@ -1506,13 +1509,16 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   const int64_t S = base->n_samples, m = base->n_snps;
   const int grid = tc_pair_blocks(ctx->tc_blocks);
   // replicates per launch: as many as fit in free device memory above 1 GiB, at most 256.
-  // Their class orders, planes and margins live in one allocation for the whole call (one
-  // allocation and one release instead of one per replicate); their genotypes and ln n!
-  // tables are the base dataset's.
+  // Their class orders, planes and margins live in one allocation for the whole call, kept
+  // afterwards as the context's spare allocation (the next call of the same shape reuses it;
+  // any other allocation of the context releases it first); their genotypes and ln n! tables
+  // are the base dataset's.
+  const auto t_call = std::chrono::steady_clock::now();
   const Layout L = dataset_layout(S, m, false);
   const size_t rep_bytes = align_up(L.total, 256);
   size_t fr = 0, tot = 0;
   CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
+  fr += ctx->spare_bytes;
   const int64_t fit = ((int64_t)fr - ((int64_t)1 << 30)) / (int64_t)rep_bytes;
   const int32_t group = (int32_t)std::max<int64_t>(1, std::min<int64_t>({fit, (int64_t)n_reps, 256}));
   int r = EPIK2_OK;
@@ -1521,14 +1527,21 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   BestSlot *d_rslots = nullptr, *d_res = nullptr;
   Rescored* d_resc = nullptr;
   char* arena = nullptr;
-  cudaError_t e = cudaMalloc(&d_jobs, sizeof(TcJob) * group);
+  size_t arena_bytes = 0;
+  cudaError_t e = take_block(ctx, rep_bytes * (size_t)group, reinterpret_cast<void**>(&arena), &arena_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&d_jobs, sizeof(TcJob) * group);
   if (e == cudaSuccess) e = cudaMalloc(&d_rslots, sizeof(BestSlot) * (size_t)group * grid);
   if (e == cudaSuccess) e = cudaMalloc(&d_res, sizeof(BestSlot) * group);
   if (e == cudaSuccess) e = cudaMalloc(&d_resc, sizeof(Rescored) * group);
-  if (e == cudaSuccess) e = cudaMalloc(&arena, rep_bytes * (size_t)group);
+  const double alloc_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count();
+  double encode_ms = 0.0;
   auto release = [&]() {
     cudaStreamSynchronize(ctx->stream);
-    cudaFree(arena);
+    if (arena) {  // becomes the context's spare allocation
+      drop_spare(ctx);
+      ctx->spare_block = arena;
+      ctx->spare_bytes = arena_bytes;
+    }
     cudaFree(d_jobs);
     cudaFree(d_rslots);
     cudaFree(d_res);
@@ -1549,6 +1562,7 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   std::vector<DevDataset> reps((size_t)group);
   for (int32_t done = 0; done < n_reps; done += group) {
     const int32_t g = std::min<int32_t>(group, n_reps - done);
+    const auto t_enc = std::chrono::steady_clock::now();
     for (int32_t t = 0; t < g; t++) {  // each replicate's class order, planes, margins
       DevDataset& R = reps[(size_t)t];
       char* b = arena + rep_bytes * (size_t)t;
@@ -1574,6 +1588,7 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
                               (int32_t)R.m_pad, (int32_t)R.w0, (int32_t)R.w1, (int32_t)R.n_controls,
                               (int32_t)R.n_cases};
     }
+    encode_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_enc).count();
     // the search's tile descriptors, after the replicates' loads (their pair margins use the
     // same descriptor buffer)
     int64_t n_tiles = 0;
@@ -1643,6 +1658,10 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   }
   release();
   ctx->stats.last_scan_kernel_ms = kms_total;
+  ctx->stats.last_load_ms = alloc_ms;
+  ctx->stats.last_prepare_ms = encode_ms;
+  ctx->stats.last_scan_wall_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count();
   ctx->stats.last_scan_triplets = triplets_before(m, m) * n_reps;
   ctx->stats.last_scan_words = 0;
   return EPIK2_OK;
