@@ -264,7 +264,7 @@ int ensure_pgoff(epik2_ctx* ctx, int64_t n) {
 int collect_topk(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, int top_k, int n_warps);
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
                 float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair,
-                bool overlap, bool a_tmem = false);
+                bool overlap);
 
 // FP4 accumulators are FP32: counts are exact below 2^24 per class.
 bool fp4_exact(const DevDataset& d) { return d.n_controls < (1 << 24) && d.n_cases < (1 << 24); }
@@ -370,11 +370,7 @@ int run_scan(epik2_ctx* ctx, DevDataset& d, const epik2_opts* opts, uint32_t* du
   int pt = (opts && opts->pair_tile) ? opts->pair_tile : ctx->pair_tile;
   int ov = (opts && opts->overlap) ? opts->overlap : ctx->overlap;
   if (pt != 0 && pt != 32 && pt != 64) return fail(ctx, EPIK2_E_INVALID, "pair_tile must be 0, 32 or 64");
-  if (ov < 0 || ov > 3) return fail(ctx, EPIK2_E_INVALID, "overlap must be 0, 1, 2 or 3");
-  if (ov == 3) {  // experiment: operand A in tensor memory (FP4, CTA pairs, 8 words per stage)
-    if (!fp4_exact(d)) return fail(ctx, EPIK2_E_TOO_LARGE, "FP4: a class of 2^24 samples or more");
-    return run_scan_tc(ctx, d, ib, ie, top_k, dump_tables, dump_scores, best_out, opts, 8, true, true, false, true);
-  }
+  if (ov < 0 || ov > 2) return fail(ctx, EPIK2_E_INVALID, "overlap must be 0, 1 or 2");
   if (engine == EPIK2_ENGINE_TC_FP4 && !fp4_exact(d))
     return fail(ctx, EPIK2_E_TOO_LARGE, "FP4 tensor-core engine: a class of 2^24 samples or more");
   const bool can_overlap = fp4_exact(d) && pipe_fits(d.n_controls, d.n_cases);
@@ -560,9 +556,8 @@ int run_pairs_tc(epik2_ctx* ctx, DevDataset& d) {
 
 // Tile descriptors of the search of first indices [ib, ie) of an m-SNP dataset into
 // ctx->d_tiles (expanded on the GPU from the pair-block list); *n_tiles receives their count.
-int prepare_tiles(epik2_ctx* ctx, int64_t m, int64_t ib, int64_t ie, bool fp4, bool pair, int64_t* n_tiles,
-                  bool a_tmem) {
-  const int64_t kk = tc_k_per_tile(fp4, a_tmem);
+int prepare_tiles(epik2_ctx* ctx, int64_t m, int64_t ib, int64_t ie, bool fp4, bool pair, int64_t* n_tiles) {
+  const int64_t kk = tc_k_per_tile(fp4);
   const int64_t jstep = pair ? 64 : 32;  // SNPs j per tile (a CTA pair takes 64)
   std::vector<uint32_t> ij;
   std::vector<int64_t> off(1, 0);
@@ -615,14 +610,13 @@ int prepare_tiles(epik2_ctx* ctx, int64_t m, int64_t ib, int64_t ie, bool fp4, b
 // 128 (int8 format) or 112 (FP4 format) SNPs.
 int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k, uint32_t* dump_tables,
                 float* dump_scores, BestSlot* best_out, const epik2_opts* opts, int kw, bool fp4, bool pair,
-                bool overlap, bool a_tmem) {
+                bool overlap) {
   const int64_t m = d.n_snps;
   pair = pair && fp4;
   overlap = overlap && pair;
-  a_tmem = a_tmem && pair && !overlap;
   const int grid = pair ? tc_pair_blocks(ctx->tc_blocks) : ctx->tc_blocks;
   int64_t n_tiles = 0;
-  int r = prepare_tiles(ctx, m, ib, ie, fp4, pair, &n_tiles, a_tmem);
+  int r = prepare_tiles(ctx, m, ib, ie, fp4, pair, &n_tiles);
   if (r) return r;
   CK(ctx, cudaMemsetAsync(ctx->d_counter, 0, 8, ctx->stream), "reset counter");
   CK(ctx, cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream), "reset error word");
@@ -654,8 +648,7 @@ int run_scan_tc(epik2_ctx* ctx, DevDataset& d, int64_t ib, int64_t ie, int top_k
   if (overlap)
     CK(ctx, launch_scan_pipe(p, grid, kw, dump_tables != nullptr, ctx->stream), "overlapped tensor-core kernel");
   else
-    CK(ctx, launch_scan_tc(p, grid, kw, fp4, pair, dump_tables != nullptr, ctx->stream, a_tmem),
-       "tensor-core scan kernel");
+    CK(ctx, launch_scan_tc(p, grid, kw, fp4, pair, dump_tables != nullptr, ctx->stream), "tensor-core scan kernel");
   CK(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream), "event");
   const int n_warps = grid * tc_warps_per_block();
   CK(ctx, launch_reduce_best(ctx->d_slots, n_warps, ctx->d_best, ctx->stream), "reduce kernel");
@@ -1118,7 +1111,7 @@ int epik2_test_withhold_arrival(epik2_ctx* ctx) {
 
 int epik2_set_overlap(epik2_ctx* ctx, int overlap) {
   if (!ctx) return EPIK2_E_INVALID;
-  if (overlap < 0 || overlap > 3) return fail(ctx, EPIK2_E_INVALID, "overlap must be 0, 1, 2 or 3");
+  if (overlap < 0 || overlap > 2) return fail(ctx, EPIK2_E_INVALID, "overlap must be 0, 1 or 2");
   ctx->overlap = overlap;
   return EPIK2_OK;
 }
@@ -1599,7 +1592,7 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
     // the search's tile descriptors, after the replicates' loads (their pair margins use the
     // same descriptor buffer)
     int64_t n_tiles = 0;
-    r = prepare_tiles(ctx, m, 0, m, true, true, &n_tiles, false);
+    r = prepare_tiles(ctx, m, 0, m, true, true, &n_tiles);
     if (r) {
       release();
       return r;

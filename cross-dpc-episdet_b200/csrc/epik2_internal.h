@@ -158,11 +158,9 @@ cudaError_t launch_rescore(const DevDataset& d, const BestSlot* cand, int64_t n,
 int scan_blocks_per_sm();
 // pair: FP4 on CTA pairs (clusters of two CTAs, tiles of 64 SNPs j); else one CTA per tile
 // of 32 SNPs j
-// a_tmem: the CTA-pair FP4 kernel with operand A in tensor memory (8 words per stage, 96 SNPs k)
 cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool pair, bool dump,
-                           cudaStream_t stream, bool a_tmem = false);
-// SNPs k per tensor-core tile: 128 (int8), 112 (FP4), 96 (FP4 with operand A in tensor memory)
-int tc_k_per_tile(bool fp4, bool a_tmem = false);
+                           cudaStream_t stream);
+int tc_k_per_tile(bool fp4);  // SNPs k per tensor-core tile: 128 (int8) or 112 (FP4)
 // The overlapped FP4 CTA-pair kernel (scan_pipe.cu): scoring of a tile runs while the next
 // tile counts; 4 or 8 words per stage; classes of at most 65535 samples (16-bit staging).
 cudaError_t launch_scan_pipe(const TcParams& p, int blocks, int words_per_stage, bool dump, cudaStream_t stream);

@@ -54,9 +54,6 @@ constexpr int kLutOff = 2 * 128 * kEStride * 4;
 constexpr int kLutCapacity = (kBarOff - kLutOff) / 4;
 static_assert(kRingBytes <= kBarOff && kLutOff % 16 == 0, "shared-memory layout");
 
-// Operand A in tensor memory (kAT): first column of A stage s (three stages of 32 columns)
-__device__ __forceinline__ uint32_t at_col(int s) { return s == 0 ? 192u : (s == 1 ? 448u : 480u); }
-
 // One dataset's view for a tile: the plain search has one, the batched search reads the
 // tile's dataset from the job table.
 struct JobView {
@@ -87,26 +84,18 @@ struct JobView {
 // pass r = 1..p.n_reps counts the cases of replicate r (p.jobs[r-1]) into the class-1
 // accumulators and scores replicate r with controls = totals - cases, its best folded into
 // p.job_slots[r-1].  Permutation replicates of one matrix thus share the all-sample counts.
-// kAT (CTA pairs, 8 words per stage): operand A in tensor memory instead of shared memory.
-// Each producing warp writes the pair-operand rows of its lane quarter (ab = warp & 3, rows
-// 32*ab + q) for two of the stage's words with tcgen05.st; only B goes through shared memory,
-// which halves the shared-memory traffic of a stage (operand stores and the tensor core's
-// operand reads).  Tensor memory then holds the two accumulators at N = 192 (96 SNPs k per
-// tile), the scale factors and a ring of three 32-column A stages: class 0 [0, 192), A stage 0
-// [192, 224), scale factors [224, 256), class 1 [256, 448), A stages 1, 2 [448, 512).
 template <int kW, bool kFp4, bool kPair, bool kBatched, bool kDump, bool kTopK, bool kMarg = false,
-          bool kRepl = false, bool kAT = false>
+          bool kRepl = false>
 __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) {
   static_assert(!kPair || kFp4, "CTA pairs use the FP4 format");
   static_assert(!kMarg || (kPair && !kBatched && !kDump && !kTopK), "pair margins: plain CTA-pair kernel");
   static_assert(!kRepl || (kPair && kW == 16 && !kBatched && !kDump && !kTopK && !kMarg), "replicates: CTA pairs");
-  static_assert(!kAT || (kPair && kW == 8 && !kMarg && !kRepl), "operand A in tensor memory: CTA pairs, 8 words");
-  constexpr int kK = kAT ? 96 : (kFp4 ? 112 : 128);  // SNPs k per tile -> 2*kK rows of B
+  constexpr int kK = kFp4 ? 112 : 128;                // SNPs k per tile -> 2*kK rows of B
   constexpr int kRowBytes = (kFp4 ? 16 : 32) * kW;    // operand bytes per row per stage
   constexpr int kBRows = kPair ? kK : 2 * kK;         // B rows held by this CTA
-  constexpr int kStageA = kAT ? 0 : 128 * kRowBytes;  // A rows in shared memory
-  constexpr int kStageBytes = kStageA + kBRows * kRowBytes;
-  constexpr int kStages = kAT ? 3 : ((kRingBytes / kStageBytes) < 4 ? (kRingBytes / kStageBytes) : 4);
+  constexpr int kStageA = 128 * kRowBytes;
+  constexpr int kStageBytes = (128 + kBRows) * kRowBytes;
+  constexpr int kStages = (kRingBytes / kStageBytes) < 4 ? (kRingBytes / kStageBytes) : 4;
   constexpr uint32_t kSbo = 8 * kRowBytes;            // bytes between 8-row groups
   constexpr int kMmas = kFp4 ? kW / 2 : kW;           // MMAs per stage (K = 64 E2M1 or 32 int8)
   constexpr int kU = kW / 4;                          // units of each kind per thread per stage
@@ -303,27 +292,6 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     const int p_k = k0 + (kK / 2) * (int)crank + p_kl;
     const uint32_t offp0 = (p_kl >> 3) * kSbo + (p_kl & 7) * 16;  // + (kK/16)*kSbo for c = 1
     const int p_wbase = tid >> 6;  // words p_wbase + 8r, r < kW/8
-    // kAT: this warp's pair-operand rows 32*ab + lane (ab = warp & 3) for words wq, wq + 1 of
-    // a stage, written to tensor-memory columns a_col(s) + 4*wq .. + 8
-    const int at_ab = warp & 3, at_wq = 2 * (warp >> 2);
-    auto load_at = [&](int cc, uint2 (&gi)[2], uint2 (&gj)[2], uint2& gk) {
-      const bool c1 = cc >= nc0;
-      const int c_in = c1 ? cc - nc0 : cc;
-      const int wcls = c1 ? lim1 : lim0;
-      const int64_t wb = (c1 ? (int64_t)jv.w0 : 0) + (int64_t)kW * c_in;
-#pragma unroll
-      for (int x = 0; x < 2; x++) {
-        gi[x] = make_uint2(0, 0);
-        gj[x] = gi[x];
-        if (kW * c_in + at_wq + x < wcls) {
-          const uint2* row = jv.planes + (wb + at_wq + x) * m_pad;
-          gi[x] = __ldg(row + i);
-          gj[x] = __ldg(row + a_j);
-        }
-      }
-      gk = make_uint2(0, 0);
-      if (kW * c_in + p_wbase < wcls && p_on && p_k < m_pad) gk = __ldg(jv.planes + (wb + p_wbase) * m_pad + p_k);
-    };
     auto load_words = [&](int cc, uint2& gi, uint2& gj, uint2 (&gk)[kUB]) {
       const bool c1 = cc >= nc0;
       const int c_in = c1 ? cc - nc0 : cc;
@@ -352,48 +320,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
         }
       }
     };
-    if (kAT && worker) {
-      uint2 ci[2], cj[2], ck;
-      if (nct > 0) load_at(0, ci, cj, ck);
-      for (int cc = 0; cc < nct; ++cc) {
-        const uint32_t g = g_chunk + (uint32_t)cc;
-        uint2 ni[2], nj[2], nk = make_uint2(0, 0);
-        ni[0] = ni[1] = nj[0] = nj[1] = nk;
-        if (cc + 1 < nct) load_at(cc + 1, ni, nj, nk);
-        const int s = (int)(g % kStages);
-        const uint32_t use = g / kStages;
-        const bool late = use > 0 && !bar_wait_cluster(bar0 + 8 * s, (use & 1u) ^ 1u, wl);
-        if (__any_sync(kFull, late)) *abort_flag = 1;
-        if (__shfl_sync(kFull, *abort_flag, 0)) break;  // warp-uniform
-        uint32_t v[8];
-#pragma unroll
-        for (int x = 0; x < 2; x++) {
-          const uint32_t wa = ((at_ab >> 1) ? ci[x].y : ci[x].x) & ((at_ab & 1) ? cj[x].y : cj[x].x);
-          const uint4 e = expand32_fp4(wa);
-          v[4 * x] = e.x;
-          v[4 * x + 1] = e.y;
-          v[4 * x + 2] = e.z;
-          v[4 * x + 3] = e.w;
-        }
-        tmem_st8(tmem + ((uint32_t)(32 * at_ab) << 16) + at_col(s) + 4 * at_wq, v);
-        if (p_on) {
-          const uint32_t offb = stage0 + s * kStageBytes + offp0 + p_wbase * 128;
-          sts128(offb, expand32_fp4(ck.x));
-          sts128(offb + (kK / 16) * kSbo, expand32_fp4(ck.y));
-        }
-#pragma unroll
-        for (int x = 0; x < 2; x++) {
-          ci[x] = ni[x];
-          cj[x] = nj[x];
-        }
-        ck = nk;
-        tmem_wait_st();
-        fence_proxy_async();
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) bar_arrive(bar_full0 + 8 * s);
-      }
-    } else if (worker) {
+    if (worker) {
       uint2 ci, cj, ck[kUB];
       if (nct > 0) load_words(0, ci, cj, ck);
       for (int cc = 0; cc < nct; ++cc) {
@@ -489,10 +416,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
 #pragma unroll
         for (int kk = 0; kk < kMmas; kk++) {  // each MMA reads 32 bytes of every row: 256 B on
           const uint32_t acc = (c_in > 0 || kk > 0) ? 1u : 0u;
-          if (kAT)
-            mma_fp4_pair_ta(d, tmem + at_col(s) + 8 * kk, db + (uint64_t)(16 * kk), acc, tmem + kSfaCol,
-                            tmem + kSfbCol);
-          else if (kPair)
+          if (kPair)
             mma_fp4_pair(d, da + (uint64_t)(16 * kk), db + (uint64_t)(16 * kk), acc, tmem + kSfaCol, tmem + kSfbCol);
           else if (kFp4)
             mma_fp4(d, da + (uint64_t)(16 * kk), db + (uint64_t)(16 * kk), acc, tmem + kSfaCol, tmem + kSfbCol);
@@ -546,19 +470,18 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     }
     for (int h = 0; h < 2; h++) {
       if (kPair) {
-        // CTA pairs: columns kK*h + (kK/2)*c + kp (kp < kK/2) hold SNP k0 + (kK/2)*h + kp,
-        // g_k = c; they go to E[cls][lane][(kK/2)*c + kp], kK/16 groups of 16 columns per class
-        // and lane quarter
+        // CTA pairs: columns 112h + 56c + kp (kp < 56) hold SNP k0 + 56h + kp, g_k = c; they
+        // go to E[cls][lane][56c + kp], 7 groups of 16 columns per class and lane quarter
 #pragma unroll
         for (int cls = 0; cls < 2; cls++) {
           const bool has = (cls ? nc1 > 0 : (kRepl || nc0 > 0)) && worker;
 #pragma unroll
           for (int t = 0; t < 2; t++) {
             const int u = cgrp + 4 * t;  // warp-uniform
-            if (u < kK / 16 && worker) {
+            if (u < 7 && worker) {
               uint32_t v[16];
               if (has) {
-                tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(cls * 256 + kK * h + 16 * u), v);
+                tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(cls * 256 + 112 * h + 16 * u), v);
                 tmem_wait_ld();
 #pragma unroll
                 for (int t2 = 0; t2 < 16; t2++) v[t2] = __float2uint_rn(__uint_as_float(v[t2]));
@@ -808,10 +731,10 @@ __global__ void k_fill_slots(BestSlot* __restrict__ slots, int64_t n) {
 
 int tc_warps_per_block() { return kTcWarps; }
 
-template <int kW, bool kF, bool kP, bool kB, bool kD, bool kT, bool kM = false, bool kR = false, bool kA = false>
+template <int kW, bool kF, bool kP, bool kB, bool kD, bool kT, bool kM = false, bool kR = false>
 static cudaError_t set_smem() {
-  return cudaFuncSetAttribute(k_scan_tc<kW, kF, kP, kB, kD, kT, kM, kR, kA>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
+  return cudaFuncSetAttribute(k_scan_tc<kW, kF, kP, kB, kD, kT, kM, kR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kTcSmemBytes);
 }
 
 template <int kW, bool kF, bool kP>
@@ -834,11 +757,6 @@ cudaError_t tc_configure() {
     if (e == cudaSuccess) e = set_smem_all<16, true, true>();
     if (e == cudaSuccess) e = set_smem<16, true, true, false, false, false, true>();         // pair margins
     if (e == cudaSuccess) e = set_smem<16, true, true, false, false, false, false, true>();  // replicates
-    // operand A in tensor memory: plain, dump, top-k and batched forms
-    if (e == cudaSuccess) e = set_smem<8, true, true, false, false, false, false, false, true>();
-    if (e == cudaSuccess) e = set_smem<8, true, true, false, true, false, false, false, true>();
-    if (e == cudaSuccess) e = set_smem<8, true, true, false, false, true, false, false, true>();
-    if (e == cudaSuccess) e = set_smem<8, true, true, true, false, false, false, false, true>();
     if (e != cudaSuccess) return e;
     configured = true;
   }
@@ -854,7 +772,7 @@ static void launch_variant(const TcParams& p, int blocks, bool batched, bool dum
 }
 
 // CTA-pair kernels: clusters of two CTAs
-template <int kW, bool kB, bool kD, bool kT, bool kM = false, bool kR = false, bool kA = false>
+template <int kW, bool kB, bool kD, bool kT, bool kM = false, bool kR = false>
 static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t stream) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)blocks);
@@ -868,19 +786,19 @@ static cudaError_t launch_pair(const TcParams& p, int blocks, cudaStream_t strea
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_scan_tc<kW, true, true, kB, kD, kT, kM, kR, kA>, p);
+  return cudaLaunchKernelEx(&cfg, k_scan_tc<kW, true, true, kB, kD, kT, kM, kR>, p);
 }
 
-template <int kW, bool kA = false>
+template <int kW>
 static cudaError_t launch_pair_variant(const TcParams& p, int blocks, bool batched, bool dump, bool topk,
                                        cudaStream_t stream) {
-  if (batched) return launch_pair<kW, true, false, false, false, false, kA>(p, blocks, stream);
-  if (dump) return launch_pair<kW, false, true, false, false, false, kA>(p, blocks, stream);
-  if (topk) return launch_pair<kW, false, false, true, false, false, kA>(p, blocks, stream);
-  return launch_pair<kW, false, false, false, false, false, kA>(p, blocks, stream);
+  if (batched) return launch_pair<kW, true, false, false>(p, blocks, stream);
+  if (dump) return launch_pair<kW, false, true, false>(p, blocks, stream);
+  if (topk) return launch_pair<kW, false, false, true>(p, blocks, stream);
+  return launch_pair<kW, false, false, false>(p, blocks, stream);
 }
 
-int tc_k_per_tile(bool fp4, bool a_tmem) { return a_tmem ? 96 : (fp4 ? 112 : 128); }
+int tc_k_per_tile(bool fp4) { return fp4 ? 112 : 128; }
 
 // CTAs of the CTA-pair kernel that can be resident at once (even; at most one per SM).
 int tc_pair_blocks(int sms) {
@@ -911,15 +829,12 @@ int tc_pair_blocks(int sms) {
 }
 
 cudaError_t launch_scan_tc(const TcParams& p, int blocks, int words_per_stage, bool fp4, bool pair, bool dump,
-                           cudaStream_t stream, bool a_tmem) {
+                           cudaStream_t stream) {
   const cudaError_t ce = tc_configure();
   if (ce != cudaSuccess) return ce;
   const bool topk = p.top_k > 1;
   const bool batched = p.jobs != nullptr;
-  if (a_tmem) {
-    const cudaError_t e = launch_pair_variant<8, true>(p, blocks & ~1, batched, dump, topk, stream);
-    if (e != cudaSuccess) return e;
-  } else if (fp4 && pair) {
+  if (fp4 && pair) {
     const cudaError_t e = words_per_stage == 16
                               ? launch_pair_variant<16>(p, blocks & ~1, batched, dump, topk, stream)
                               : launch_pair_variant<8>(p, blocks & ~1, batched, dump, topk, stream);

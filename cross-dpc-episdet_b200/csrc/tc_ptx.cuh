@@ -15,10 +15,6 @@ constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) 
 constexpr uint32_t kIdescFp4 = (1u << 7) | (1u << 10) | ((224u >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
 // the same for a CTA pair (cta_group::2): M = 256, each CTA holding 128 rows of A, 112 of B
 constexpr uint32_t kIdescFp4Pair = (1u << 7) | (1u << 10) | ((224u >> 3) << 17) | (1u << 23) | ((256u >> 4) << 24);
-// the same with N = 192 (96 SNPs k per tile): the CTA-pair kernel that keeps operand A in
-// tensor memory
-constexpr uint32_t kIdescFp4PairN192 =
-    (1u << 7) | (1u << 10) | ((192u >> 3) << 17) | (1u << 23) | ((256u >> 4) << 24);
 // FP4 format: TMEM columns [224, 256) hold the scale factors (all 2^1), A's from 224 (4
 // columns), B's from 240 (8 columns); class 0 accumulates into [0, 224), class 1 into
 // [256, 480).
@@ -62,12 +58,6 @@ __device__ __forceinline__ void tmem_st16_fill(uint32_t addr, uint32_t v) {
       "r"(v)
       : "memory");
 }
-// 8 consecutive columns of this thread's lane (the warp's lane quarter is in addr)
-__device__ __forceinline__ void tmem_st8(uint32_t addr, const uint32_t (&v)[8]) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(addr), "r"(v[0]),
-               "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
-               : "memory");
-}
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // CTA-pair forms.  The MMA is issued by the even CTA of a cluster of two; each CTA's shared
@@ -81,18 +71,6 @@ __device__ __forceinline__ void mma_fp4_pair(uint32_t d_tmem, uint64_t a, uint64
       "tcgen05.mma.cta_group::2.kind::mxf4.block_scale.scale_vec::2X [%0], %1, %2, %3, [%5], [%6], p;\n\t}\n" ::"r"(
           d_tmem),
       "l"(a), "l"(b), "r"(kIdescFp4Pair), "r"(accumulate), "r"(sfa_tmem), "r"(sfb_tmem));
-}
-// The same with operand A read from tensor memory (each CTA's 128 rows in its own tensor
-// memory at a_tmem: row r in lane r, 64 E2M1 values = 8 columns, sample 8c + e in bits
-// [4e, 4e + 4) of column c) and N = 192.
-__device__ __forceinline__ void mma_fp4_pair_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t accumulate,
-                                                uint32_t sfa_tmem, uint32_t sfb_tmem) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::2.kind::mxf4.block_scale.scale_vec::2X [%0], [%1], %2, %3, [%5], [%6], p;\n\t}\n" ::"r"(
-          d_tmem),
-      "r"(a_tmem), "l"(b), "r"(kIdescFp4PairN192), "r"(accumulate), "r"(sfa_tmem), "r"(sfb_tmem));
 }
 // arrive on the mbarrier at this offset in both CTAs of the pair once the MMAs complete
 __device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
