@@ -683,7 +683,9 @@ def serving_form(seconds=15.0, drain=15.0, check_requests=6):
                                               "median": float(np.median(errs)) if errs else None,
                                               "results": len(errs)},
                 "scans_done": st["scans_done"], "launches": st["launches"], "max_scans_per_launch": st["max_active"],
-                "busy_fraction": st["busy_seconds"] / wall}, done
+                "busy_fraction": st["busy_seconds"] / wall,
+                "kernel_fraction_of_busy": st["kernel_seconds"] / max(st["busy_seconds"], 1e-9),
+                "replicate_form_scans": st["replicate_scans"]}, done
 
     def full_request(mids):
         if rng.random() < spec["upload_frac"]:

@@ -67,6 +67,12 @@ struct epik2_ctx {
   // pointer: the job table is rewritten before every replay), least recently used first
   std::map<std::vector<int64_t>, std::unique_ptr<struct BatchPlan>> plans;
   std::vector<std::vector<int64_t>> plan_lru;
+  // replicate form scratch: job table, per-CTA slots, results (grown, never shrunk)
+  TcJob* d_rep_jobs = nullptr;
+  BestSlot* d_rep_slots = nullptr;
+  BestSlot* d_rep_res = nullptr;
+  Rescored* d_rep_resc = nullptr;
+  int64_t rep_cap = 0, rep_slot_cap = 0;
 };
 
 constexpr size_t kMaxPlans = 32;  // cached batched plans per context
@@ -1050,6 +1056,10 @@ void epik2_destroy(epik2_ctx* ctx) {
   cudaFree(ctx->d_pb_off);
   cudaFree(ctx->d_pb_ij);
   cudaFree(ctx->d_tiles);
+  cudaFree(ctx->d_rep_jobs);
+  cudaFree(ctx->d_rep_slots);
+  cudaFree(ctx->d_rep_res);
+  cudaFree(ctx->d_rep_resc);
   cudaFreeHost(ctx->h_best);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
@@ -1523,16 +1533,41 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   const int32_t group = (int32_t)std::max<int64_t>(1, std::min<int64_t>({fit, (int64_t)n_reps, 256}));
   int r = EPIK2_OK;
   const bool rescore = opts && opts->rescore_fp64;
-  TcJob* d_jobs = nullptr;
-  BestSlot *d_rslots = nullptr, *d_res = nullptr;
-  Rescored* d_resc = nullptr;
   char* arena = nullptr;
   size_t arena_bytes = 0;
-  cudaError_t e = take_block(ctx, rep_bytes * (size_t)group, reinterpret_cast<void**>(&arena), &arena_bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&d_jobs, sizeof(TcJob) * group);
-  if (e == cudaSuccess) e = cudaMalloc(&d_rslots, sizeof(BestSlot) * (size_t)group * grid);
-  if (e == cudaSuccess) e = cudaMalloc(&d_res, sizeof(BestSlot) * group);
-  if (e == cudaSuccess) e = cudaMalloc(&d_resc, sizeof(Rescored) * group);
+  cudaError_t e = cudaSuccess;
+  const size_t need = rep_bytes * (size_t)group;
+  if (ctx->spare_block && ctx->spare_bytes >= need) {  // a larger spare serves too: it is returned
+    arena = static_cast<char*>(ctx->spare_block);
+    arena_bytes = ctx->spare_bytes;
+    ctx->spare_block = nullptr;
+    ctx->spare_bytes = 0;
+  } else {
+    e = take_block(ctx, need, reinterpret_cast<void**>(&arena), &arena_bytes);
+  }
+  if (e == cudaSuccess && (group > ctx->rep_cap || (int64_t)group * grid > ctx->rep_slot_cap)) {
+    cudaFree(ctx->d_rep_jobs);
+    cudaFree(ctx->d_rep_slots);
+    cudaFree(ctx->d_rep_res);
+    cudaFree(ctx->d_rep_resc);
+    ctx->d_rep_jobs = nullptr;
+    ctx->d_rep_slots = nullptr;
+    ctx->d_rep_res = nullptr;
+    ctx->d_rep_resc = nullptr;
+    ctx->rep_cap = ctx->rep_slot_cap = 0;
+    const int64_t cap = std::max<int64_t>(group, 64);
+    e = cudaMalloc(&ctx->d_rep_jobs, sizeof(TcJob) * cap);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_rep_slots, sizeof(BestSlot) * (size_t)cap * grid);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_rep_res, sizeof(BestSlot) * cap);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_rep_resc, sizeof(Rescored) * cap);
+    if (e == cudaSuccess) {
+      ctx->rep_cap = cap;
+      ctx->rep_slot_cap = cap * grid;
+    }
+  }
+  TcJob* d_jobs = ctx->d_rep_jobs;
+  BestSlot *d_rslots = ctx->d_rep_slots, *d_res = ctx->d_rep_res;
+  Rescored* d_resc = ctx->d_rep_resc;
   const double alloc_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count();
   double encode_ms = 0.0;
   auto release = [&]() {
@@ -1542,10 +1577,6 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
       ctx->spare_block = arena;
       ctx->spare_bytes = arena_bytes;
     }
-    cudaFree(d_jobs);
-    cudaFree(d_rslots);
-    cudaFree(d_res);
-    cudaFree(d_resc);
   };
   if (e != cudaSuccess) {
     release();

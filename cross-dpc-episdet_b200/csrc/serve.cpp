@@ -163,6 +163,8 @@ struct epik2_server {
       std::vector<epik2_best> res;
       std::vector<epik2_best> rep_res(batch.size());
       std::vector<char> in_rep(batch.size(), 0);  // scanned in the replicate form
+      double kernel_s = 0.0;                       // device time of this launch's search kernels
+      int64_t rep_scans = 0;
       for (int spin = 0; spin < 1000 && ctx_waiters.load() > 0; spin++)  // let add_matrix in first
         std::this_thread::sleep_for(std::chrono::microseconds(100));
       {
@@ -184,6 +186,12 @@ struct epik2_server {
           epik2_opts o{};
           o.rescore_fp64 = opts.rescore_fp64;
           const int st = epik2_scan_replicates(ctx, kv.first, ph.data(), (int32_t)kv.second.size(), &o, out.data());
+          if (st == EPIK2_OK) {
+            epik2_stats cs{};
+            epik2_get_stats(ctx, &cs);
+            kernel_s += cs.last_scan_kernel_ms * 1e-3;
+            rep_scans += (int64_t)kv.second.size();
+          }
           for (size_t t = 0; t < kv.second.size(); t++) {
             status[kv.second[t]] = st;
             rep_res[kv.second[t]] = out[t];
@@ -211,6 +219,11 @@ struct epik2_server {
           const int st = epik2_scan_batch(ctx, ids.data(), (int32_t)ids.size(), &o, res.data());
           if (st != EPIK2_OK)
             for (size_t t : ok_items) status[t] = st;
+          else {
+            epik2_stats cs{};
+            epik2_get_stats(ctx, &cs);
+            kernel_s += cs.last_scan_kernel_ms * 1e-3;
+          }
         }
         for (int32_t id : ids) epik2_unload(ctx, id);
       }
@@ -219,6 +232,8 @@ struct epik2_server {
         std::lock_guard<std::mutex> lk(mu);
         stats.launches++;
         stats.busy_seconds += dt;
+        stats.kernel_seconds += kernel_s;
+        stats.replicate_scans += rep_scans;
         size_t q = 0;
         for (size_t b = 0; b < batch.size(); b++) {
           Request* r = batch[b].req;

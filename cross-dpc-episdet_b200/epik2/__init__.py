@@ -84,7 +84,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("rejected", ctypes.c_int64),
                 ("cancelled", ctypes.c_int64), ("scans_queued", ctypes.c_int64), ("scans_active", ctypes.c_int64),
                 ("scans_done", ctypes.c_int64), ("launches", ctypes.c_int64), ("triplet_samples", ctypes.c_double),
-                ("busy_seconds", ctypes.c_double), ("max_active", ctypes.c_int64)]
+                ("busy_seconds", ctypes.c_double), ("max_active", ctypes.c_int64),
+                ("kernel_seconds", ctypes.c_double), ("replicate_scans", ctypes.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -303,6 +303,8 @@ typedef struct {
   double triplet_samples; /* completed work */
   double busy_seconds;    /* worker time inside batched launches */
   int64_t max_active;     /* most scans admitted to one launch so far */
+  double kernel_seconds;  /* device time of the search kernels inside those launches */
+  int64_t replicate_scans;/* scans that ran in the replicate form (epik2_scan_replicates) */
 } epik2_server_stats;
 int epik2_server_create(epik2_server **out, int device, const epik2_server_opts *opts);
 void epik2_server_destroy(epik2_server *srv);
