@@ -88,3 +88,24 @@ def test_early_tiles_of_the_queue_are_searched():
     assert got[0].ijk == (2, 5, 40)
     for a, b in zip(got, plain):
         assert a.ijk == b.ijk and f32_bits(a.score) == f32_bits(b.score)
+
+
+def test_fp64_rescore_of_each_replicate_equals_oracle():
+    """With rescore_fp64 each replicate's best carries its FP64 K2 score, computed on the GPU
+    from the replicate's own tables: equal bit for bit to the oracle's FP64 K2 of that
+    triplet's table under the replicate's phenotype, and to the plain search's rescore."""
+    g, p = O.gen_hwe(137, 900, 60, 420, planted=[(4, 30, 55)], effects=[0.7])
+    reps = np.concatenate([p[None, :], _perms(p, 5, 137)])
+    with epik2.Context(0) as ctx:
+        base = ctx.load(g, p)
+        got = ctx.scan_replicates(base, reps, rescore_fp64=1)
+        plain = []
+        for r in reps:
+            ctx.set_pheno(base, r)
+            plain.append(ctx.scan(base, engine=epik2.ENGINE_TC_FP4, stage_words=16, pair_tile=64, overlap=1,
+                                  rescore_fp64=1))
+        ctx.unload(base)
+    for r, a, b in zip(reps, got, plain):
+        assert a.ijk == b.ijk and f32_bits(a.score) == f32_bits(b.score)
+        assert a.score_fp64 == b.score_fp64
+        assert a.score_fp64 == O.k2_fp64(O.table(g, r, *a.ijk))
