@@ -589,6 +589,8 @@ def replicates_form(n_a=64, n_b=8):
     rng = np.random.default_rng(1006)
     with epik2.Context(0) as ctx:
         for m, n in zip(W.SERVING["resident"], (n_a, n_b)):
+            if n <= 0:
+                continue
             g, p = W.generate(m)
             reps = np.stack([rng.permutation(p) for _ in range(n)])
             did = ctx.load(g, p)
@@ -775,7 +777,9 @@ def main():
     ap.add_argument("--flush-mb", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="plain", choices=["plain", "batched", "precision", "serving"])
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "precision", "serving", "replicates"])
+    ap.add_argument("--replicates", default="64,8",
+                    help="replicates form: replicates of serving matrices A and B (0 leaves a matrix out)")
     ap.add_argument("--engine", default="auto", choices=["auto", "int", "tc", "fp4"],
                     help="plain form: search engine (default: the autotuner's choice)")
     ap.add_argument("--stage-words", type=int, default=0, help="plain form: tensor-core stage depth (0 = tuned)")
@@ -795,6 +799,10 @@ def main():
         return run_precision(args)
     if args.form == "serving":
         return run_serving(args)
+    if args.form == "replicates":
+        n_a, n_b = (int(x) for x in args.replicates.split(","))
+        print(json.dumps({"form": "replicates", "data": "synthetic", "replicates": replicates_form(n_a, n_b)}))
+        return 0
     return run_ours(args, rank, world, local_rank)
 
 
