@@ -422,8 +422,8 @@ def run_ours(args, rank, world, local_rank):
     ctx.close()
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
-        # the other forms of the north star, bounded (about 1.5 minutes together), after the
-        # timed region: batched, precision and serving
+        # the other forms, bounded (about 1.5 minutes together), after the timed region:
+        # precision, batched, replicates and serving
         forms = {}
         for name, fn in (("precision", precision_form), ("batched", batched_form), ("replicates", replicates_form),
                          ("serving", serving_form)):
