@@ -109,3 +109,35 @@ def test_fp64_rescore_of_each_replicate_equals_oracle():
         assert a.ijk == b.ijk and f32_bits(a.score) == f32_bits(b.score)
         assert a.score_fp64 == b.score_fp64
         assert a.score_fp64 == O.k2_fp64(O.table(g, r, *a.ijk))
+
+
+def test_spare_allocation_shared_with_the_one_call_entry_point():
+    """The replicates' allocation stays with the context as its spare (reported as free) and
+    serves or yields to the next allocation: one-call scans before and after a replicate call,
+    and a second replicate call of another shape, all keep their results, and the context's
+    free memory (spare included) returns to where it was."""
+    g, p = O.gen_hwe(138, 800, 50, 380)
+    g2, p2 = O.gen_hwe(139, 1500, 90, 700)
+    reps = _perms(p, 12, 138)
+    with epik2.Context(0) as ctx:
+        free0 = ctx.mem_info()[0]
+        a = ctx.scan_u8(g, p)
+        base = ctx.load(g, p)
+        got = ctx.scan_replicates(base, reps)
+        b = ctx.scan_u8(g2, p2)
+        base2 = ctx.load(g2, p2)
+        got2 = ctx.scan_replicates(base2, _perms(p2, 3, 139))
+        ctx.unload(base2)
+        again = ctx.scan_replicates(base, reps[:5])
+        ctx.unload(base)
+        free1 = ctx.mem_info()[0]
+    ref, ref2 = O.scan(g, p), O.scan(g2, p2)
+    assert a.ijk == ref["ijk"] and f32_bits(a.score) == f32_bits(ref["score"])
+    assert b.ijk == ref2["ijk"] and f32_bits(b.score) == f32_bits(ref2["score"])
+    for r, x in zip(reps[:3], got[:3]):
+        rr = O.scan(g, r)
+        assert x.ijk == rr["ijk"] and f32_bits(x.score) == f32_bits(rr["score"])
+    assert [x.ijk for x in again] == [x.ijk for x in got[:5]]
+    assert [f32_bits(x.score) for x in again] == [f32_bits(x.score) for x in got[:5]]
+    assert len(got2) == 3
+    assert abs(free1 - free0) < (64 << 20)  # scratch of a few MiB may stay allocated
