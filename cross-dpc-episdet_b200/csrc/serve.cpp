@@ -6,7 +6,7 @@
 // turn (round robin from where the previous round stopped, so a small request is not held
 // behind a large one); create each admitted scan's dataset (a replicate sharing a
 // resident genotype matrix, or a freshly uploaded matrix); run one batched launch over
-// all of them (epik2_scan_batch) -- except that two or more replicates of one resident matrix
+// all of them (epik2_scan_batch) -- except that three or more replicates of one resident matrix
 // admitted together run in the replicate form (epik2_scan_replicates: each tile's all-sample
 // counts shared by them); release the datasets; and complete the requests whose scans are
 // all done.  Requests that arrive during a launch join the next admission
@@ -169,13 +169,14 @@ struct epik2_server {
         std::this_thread::sleep_for(std::chrono::microseconds(100));
       {
         std::lock_guard<std::mutex> g(ctx_mu);
-        // replicate scans of one resident matrix (two or more in this launch) run in the
-        // replicate form: each tile's all-sample counts are shared by the replicates
+        // replicate scans of one resident matrix run in the replicate form (each tile's
+        // all-sample counts shared by the replicates) when this launch holds three or more of
+        // them: below that the all-sample pass costs about what it saves
         std::map<int32_t, std::vector<size_t>> by_matrix;
         for (size_t b = 0; b < batch.size(); b++)
           if (batch[b].req->dataset >= 0) by_matrix[batch[b].req->dataset].push_back(b);
         for (auto& kv : by_matrix) {
-          if (kv.second.size() < 2 || batch[kv.second[0]].req->n_samples >= (1 << 24)) continue;
+          if (kv.second.size() < 3 || batch[kv.second[0]].req->n_samples >= (1 << 24)) continue;
           const size_t s_n = (size_t)batch[kv.second[0]].req->n_samples;
           std::vector<uint8_t> ph(kv.second.size() * s_n);
           for (size_t t = 0; t < kv.second.size(); t++) {
