@@ -64,8 +64,8 @@ static_assert(PipeShape<4>::kLutCap % 4 == 0 && PipeShape<8>::kLutCap % 4 == 0, 
 static_assert(PipeShape<4>::kLutCap >= 16388, "16384 samples keep their table in shared memory");
 
 // barrier slots (8 bytes each) at kPipeBarOff
-constexpr int kBFull = 0, kBEmpty = 4, kBAcc = 8, kBTile = 9, kBDrained = 13, kBDesc = 14;
-static_assert((kBDesc + 4) * 8 <= 256, "barrier area");
+constexpr int kBFull = 0, kBEmpty = 4, kBAcc = 8, kBTile = 9, kBDrained = 13, kBDesc = 14, kBFinal = 18;
+static_assert((kBFinal + 1) * 8 <= 256, "barrier area");
 
 // One dataset's view for a tile (the batched form reads the tile's dataset from the job table).
 struct JobRef {
@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_scan_pipe(const TcParams p)
       bar_init(bar(kBDesc + d), 1);
     }
     bar_init(bar(kBDrained), 8 + (even ? 1 : 0));
+    bar_init(bar(kBFinal), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
     s_pfail = 0;
@@ -523,7 +524,14 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_scan_pipe(const TcParams p)
     }
   }
 
-  // ---- teardown: every role has left its loop; the last tile's products were waited for ----
+  // ---- teardown: every role has left its loop ----
+  // Tensor memory is released only after every product has completed (after an expired wait
+  // the issuer may have left its last stages running): the issuing lane commits once more and
+  // each CTA's lane 0 of the issuing warp waits for that commit, bounded.
+  if (warp == 16 && lane == 0) {
+    if (even) mma_commit_pair(bar(kBFinal));
+    if (!bar_wait_cluster(bar(kBFinal), 0, wl)) s_abort = 1;
+  }
   tc_fence_before();
   __syncthreads();
   if ((s_abort || s_pfail || s_sfail) && tid == 0) atomicExch(p.err, 1);

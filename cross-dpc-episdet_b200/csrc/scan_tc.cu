@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
   const uint32_t bar_acc = bar0 + 8 * kStages;
   const uint32_t bar_full0 = bar_acc + 8;  // [stages]: one arrival per producing warp (+1 forwarded)
   const uint32_t bar_tile = bar_full0 + 8 * kStages;  // CTA pairs: the odd CTA's "next tile is set"
+  const uint32_t bar_final = bar_tile + 8;  // the issuer's last commit: every product has completed
   volatile int* abort_flag = &s_abort;
   const bool worker = warp < kTcWarps;
   const long long wl = p.wait_limit > 0 ? p.wait_limit : kWaitLimit;  // clocks a bounded wait lasts
@@ -130,6 +131,7 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     // full: the CTA's producing warps, and in a pair's issuing CTA one forwarded arrival
     for (int s = 0; s < kStages; s++) bar_init(bar_full0 + 8 * s, kTcWarps + ((kPair && crank == 0) ? 1 : 0));
     bar_init(bar_tile, 1);
+    bar_init(bar_final, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
   }
@@ -619,7 +621,18 @@ __global__ void __launch_bounds__(kTcThreadsAll, 1) k_scan_tc(const TcParams p) 
     if (*abort_flag) break;
   }
 
-  // ---- teardown: every MMA has completed (its tile's accumulator barrier was waited) ----
+  // ---- teardown ----
+  // Tensor memory is released only after every product has completed.  A search that ran to
+  // its end waited for each tile's products already; after an expired wait the issuer may
+  // have left its last stages running.  So the issuing thread commits once more and that
+  // commit is waited for (bounded) in each CTA it arrives in.
+  if (!worker && lane == 0) {
+    if (issuer_cta) {
+      if (kPair) mma_commit_pair(bar_final);
+      else mma_commit(bar_final);
+    }
+    if (!(kPair ? bar_wait_cluster(bar_final, 0, wl) : bar_wait(bar_final, 0, wl))) *abort_flag = 1;
+  }
   tc_fence_before();
   __syncthreads();
   if (s_abort && tid == 0) atomicExch(p.err, 1);
