@@ -1186,10 +1186,15 @@ int epik2_load_u8(epik2_ctx* ctx, const uint8_t* geno, const uint8_t* pheno, int
     return fail(ctx, EPIK2_E_TOO_LARGE, "n_samples or n_snps beyond limit");
   CK(ctx, cudaSetDevice(ctx->device), "set device");
   const Layout L = dataset_layout(n_samples, n_snps);
-  size_t fr = 0, tot = 0;
-  CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
-  if (L.total + (size_t)(256u << 20) > fr + ctx->spare_bytes)
-    return fail(ctx, EPIK2_E_NOMEM, "dataset does not fit in free device memory");
+  // the spare allocation serves when it fits without doubling the footprint (take_block):
+  // then nothing new is allocated and free memory need not be asked for
+  const bool reuse = ctx->spare_block && ctx->spare_bytes >= L.total && ctx->spare_bytes <= 2 * L.total;
+  if (!reuse) {
+    size_t fr = 0, tot = 0;
+    CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
+    if (L.total + (size_t)(256u << 20) > fr + ctx->spare_bytes)
+      return fail(ctx, EPIK2_E_NOMEM, "dataset does not fit in free device memory");
+  }
   std::unique_ptr<DevDataset> d(new DevDataset());
   CK(ctx, take_block(ctx, L.total, &d->block, &d->block_bytes), "alloc dataset");
   char* b = (char*)d->block;
