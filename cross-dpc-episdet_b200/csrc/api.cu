@@ -1277,10 +1277,12 @@ int epik2_load_replicate(epik2_ctx* ctx, int32_t base_dataset_id, const uint8_t*
   if (!root) return fail(ctx, EPIK2_E_NOT_FOUND, "genotype owner no longer loaded");
   CK(ctx, cudaSetDevice(ctx->device), "set device");
   const Layout L = dataset_layout(root->n_samples, root->n_snps, false);
-  size_t fr = 0, tot = 0;
-  CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
-  if (L.total + (size_t)(256u << 20) > fr + ctx->spare_bytes)
-    return fail(ctx, EPIK2_E_NOMEM, "replicate does not fit in free device memory");
+  if (!(ctx->spare_block && ctx->spare_bytes >= L.total && ctx->spare_bytes <= 2 * L.total)) {
+    size_t fr = 0, tot = 0;  // a new allocation: ask for free memory (about a millisecond)
+    CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
+    if (L.total + (size_t)(256u << 20) > fr + ctx->spare_bytes)
+      return fail(ctx, EPIK2_E_NOMEM, "replicate does not fit in free device memory");
+  }
   std::unique_ptr<DevDataset> d(new DevDataset());
   CK(ctx, take_block(ctx, L.total, &d->block, &d->block_bytes), "alloc replicate");
   char* b = (char*)d->block;
@@ -1531,11 +1533,15 @@ int epik2_scan_replicates(epik2_ctx* ctx, int32_t dataset_id, const uint8_t* phe
   const auto t_call = std::chrono::steady_clock::now();
   const Layout L = dataset_layout(S, m, false);
   const size_t rep_bytes = align_up(L.total, 256);
-  size_t fr = 0, tot = 0;
-  CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
-  fr += ctx->spare_bytes;
-  const int64_t fit = ((int64_t)fr - ((int64_t)1 << 30)) / (int64_t)rep_bytes;
-  const int32_t group = (int32_t)std::max<int64_t>(1, std::min<int64_t>({fit, (int64_t)n_reps, 256}));
+  const int64_t want = std::min<int64_t>(n_reps, 256);
+  int64_t fit = want;  // a spare allocation that holds them all needs no free-memory query
+  if (!(ctx->spare_block && ctx->spare_bytes >= rep_bytes * (size_t)want)) {
+    size_t fr = 0, tot = 0;
+    CK(ctx, cudaMemGetInfo(&fr, &tot), "mem info");
+    fr += ctx->spare_bytes;
+    fit = ((int64_t)fr - ((int64_t)1 << 30)) / (int64_t)rep_bytes;
+  }
+  const int32_t group = (int32_t)std::max<int64_t>(1, std::min<int64_t>(fit, want));
   int r = EPIK2_OK;
   const bool rescore = opts && opts->rescore_fp64;
   char* arena = nullptr;
